@@ -1,0 +1,450 @@
+#!/usr/bin/env python
+"""Benchmark of the closed-form matting hot path on B200.
+
+Workload (one "step"): a seeded synthetic 1920x1080 image with ~10%
+scribbles (eps = 1e-5, gamma = 100) goes through the hot path: FP64 Levin
+Laplacian assembly into the FP16 symmetric band store, then the fused
+persistent mixed-precision CG to relative residual 1e-6 (FP64 true-residual
+replacement every 50 iterations, max 5000).  The metric is Mpix * CG
+iterations per second over the whole job; ms_per_step is the time to
+relative residual 1e-6.
+
+  value   device-resident inputs, CUDA events on the launching stream, L2
+          flushed (256 MB write) between timed steps.
+  e2e     the same step through the C ABI from pinned HOST buffers: H2D of the
+          RGB8 image, scribbles and initial alpha, assembly, solve, D2H alpha.
+  plain   (N=1, rank 0) the plain FP32 method on the same image: 25-band FP32
+          reference-layout store, fused CG, same stopping rule.
+
+Multi-GPU: one process per GPU (torchrun); every rank solves its own image
+(seed = rank), no data-path collective; time is the max over ranks.
+
+--impl reference times the reference's own CPU path (hostLevinLaplacian +
+gaussSeidel_host from oracle/_ref, compiled from the reference sources) on the
+same image with all host threads, one independent image per thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpix·CG-iter/s and time to rel-residual 1e-6 at 1080p, mixed vs FP32, 1 B200"
+UNIT = "Mpix·CG-iter/s"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+# Algorithmic bytes per pixel: Krylov sweep of the FP16
+# symmetric store = 12 planes x 2 B + gamma 4 B + read r,q,p 12 B + write
+# r,p,q 12 B + solution increment read/write 8 B.
+KRYLOV_BYTES = {"fp16": 60, "bf16": 60, "fp32": 84, "ref25": 132}
+REPLACE_BYTES = {"sym_mixed": 92, "ref25": 124}
+IMPORT_BYTES = {"sym_mixed": 36, "ref25": 20}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        d["source"] = "measured"
+        return d
+    return dict(FALLBACK_PEAKS)
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", self.gpu_id], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU path
+# ---------------------------------------------------------------------------
+def reference_cpu_path(prob, sweeps: int, threads: int, steps: int = 1):
+    """hostLevinLaplacian + `sweeps` gaussSeidel_host sweeps per image, one
+    image per thread; returns (seconds per step list, kind, assembly_s)."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    W, H = prob.W, prob.H
+    N = W * H
+    im4 = prob.image_float4()
+    offs = O.levin_offsets(W)
+
+    def one(out: list):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            a, b = O.ref_levin(im4, prob.scribbles, prob.eps)
+        else:
+            a, b = O.levin_ref32(im4, prob.scribbles, prob.eps, 1.0)
+        t1 = time.perf_counter()
+        x = np.full(N, 0.5, np.float32)
+        O.gs_host(a, offs, b, x, sweeps, use_ref=(kind == "reference"))
+        t2 = time.perf_counter()
+        out.append((t1 - t0, t2 - t1))
+
+    times, asm = [], []
+    for _ in range(steps):
+        outs: list = []
+        ths = [threading.Thread(target=one, args=(outs,)) for _ in range(threads)]
+        t0 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        times.append(time.perf_counter() - t0)
+        asm.append(statistics.mean(o[0] for o in outs))
+    return times, kind, statistics.mean(asm)
+
+
+def calibrate_sweeps(prob, target_s: float) -> int:
+    """Gauss-Seidel sweeps that take about target_s on one core."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    W, H = prob.W, prob.H
+    a, b = O.levin_ref32(prob.image_float4(), prob.scribbles, prob.eps, 1.0)
+    x = np.full(W * H, 0.5, np.float32)
+    t0 = time.perf_counter()
+    O.gs_host(a, O.levin_offsets(W), b, x, 2)
+    per = (time.perf_counter() - t0) / 2
+    return max(1, int(target_s / max(per, 1e-6)))
+
+
+def cpu_threads_for(W: int, H: int) -> int:
+    n = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
+    except (ValueError, OSError):
+        avail = 16 << 30
+    per = 40 * W * H * 4  # bands, rhs, x, image per thread
+    return max(1, min(n, int(0.5 * avail // per)))
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from gpumatting_b200.synth import make_problem
+
+    prob = make_problem(args.W, args.H, 0)
+    threads = cpu_threads_for(args.W, args.H)
+    sweeps = calibrate_sweeps(prob, args.ref_seconds)
+    reference_cpu_path(prob, sweeps, threads, steps=args.warmup)
+    times, kind, asm = reference_cpu_path(prob, sweeps, threads, steps=args.steps)
+    N = args.W * args.H
+    total = sum(times)
+    value = threads * N * sweeps * args.steps / 1e6 / total
+    sample = (f"{args.W}x{args.H} image per thread: hostLevinLaplacian ({asm:.2f} s) + {sweeps} gaussSeidel_host "
+              f"sweeps, {threads} independent images on {threads} threads")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "iterations are Gauss-Seidel sweeps (Solve.cpp:3-33); the reference has no CPU CG"}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args) -> dict:
+    return {"workload": f"{args.W}x{args.H} synthetic matting solve (seeded), eps=1e-5, gamma=100, ~10% scribbles; "
+                        f"{args.precision.upper()} symmetric band store, fused mixed CG to rel-residual 1e-6 "
+                        f"(FP64 replacement every 50, max 5000)",
+            "W": args.W, "H": args.H, "precision": args.precision, "rtol": 1e-6,
+            "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from gpumatting_b200 import _lib as L
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
+
+    world, rank, local = dist_setup()
+    W, H = args.W, args.H
+    N = W * H
+    prob = make_problem(W, H, rank)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    img_h = torch.from_numpy(prob.image).pin_memory()
+    scr_h = torch.from_numpy(prob.scribbles).pin_memory()
+    a0_h = torch.full((H, W), 0.5, dtype=torch.float32).pin_memory()
+    out_h = torch.empty((H, W), dtype=torch.float32).pin_memory()
+    img_d = img_h.to(dev)
+    scr_d = scr_h.to(dev)
+    a0_d = a0_h.to(dev)
+    alpha = torch.empty((H, W), dtype=torch.float32, device=dev)
+    store = api.LevinStore(W, H, args.precision)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MB > L2
+    params = dict(rtol=1e-6, max_iters=5000, replace_every=50)
+
+    def step_device():
+        store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
+        alpha.copy_(a0_d, non_blocking=True)
+        return store.solve(alpha, "cg", **params)
+
+    def step_e2e():
+        img_d.copy_(img_h, non_blocking=True)
+        scr_d.copy_(scr_h, non_blocking=True)
+        alpha.copy_(a0_h, non_blocking=True)
+        store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
+        r = store.solve(alpha, "cg", **params)
+        out_h.copy_(alpha, non_blocking=True)
+        return r
+
+    def timed(fn, k):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        res = []
+        for i in range(k):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            res.append(fn())
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in ev], res
+
+    for _ in range(args.warmup):
+        r = step_device()
+        assert r.status == 0, r
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    clocks = ClockSampler(gpu_id)
+    barrier(world)
+    clocks.start()
+    ms, res = timed(step_device, args.steps)
+    barrier(world)
+    clk = clocks.stop()
+    for r in res:
+        assert r.status == 0 and r.rel_residual <= 1e-6, r
+    iters = sum(r.iters for r in res)
+    reps = sum(r.replacements for r in res)
+    kern_ms = sum(r.kernel_ms for r in res)
+    t_local = sum(ms) / 1000.0
+    t_max = allreduce_max(t_local, world)
+    work = allreduce_sum(N * iters, world)
+    value = work / 1e6 / t_max
+
+    # e2e through the C ABI with host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    barrier(world)
+    ms_e, res_e = timed(step_e2e, args.steps)
+    barrier(world)
+    iters_e = sum(r.iters for r in res_e)
+    te_max = allreduce_max(sum(ms_e) / 1000.0, world)
+    e2e_value = allreduce_sum(N * iters_e, world) / 1e6 / te_max
+
+    peaks = load_peaks()
+    kb = KRYLOV_BYTES[args.precision]
+    alg_bytes = N * (iters * kb + reps * REPLACE_BYTES["sym_mixed"] + args.steps * IMPORT_BYTES["sym_mixed"])
+    achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "solver_traffic.json")
+    if os.path.exists(tr_path):
+        tr = json.load(open(tr_path))
+        if tr.get("precision") == args.precision and tr.get("W") == W and tr.get("H") == H:
+            traffic = tr["dram_bytes_per_px_iter"] * N * iters / args.steps
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.precision + " bands / f32 vectors / f64 residual",
+            "data": "synthetic", "config": config_dict(args),
+            "time_to_rtol_ms": 1000 * t_max / args.steps,
+            "iters_per_solve": iters / args.steps, "replacements_per_solve": reps / args.steps,
+            "solver_kernel_ms": kern_ms / args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                         "peak_source": peaks.get("source"),
+                         "alg_bytes_per_launch": alg_bytes / args.steps,
+                         "kernel": "gm::solver_kernel (fused persistent CG)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * (3 + 1 + 4),
+                    "d2h_bytes_per_step": N * 4, "ms_per_step": 1000 * te_max / args.steps},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_plain:
+        line["plain_fp32"] = run_plain(args, prob, img_d, scr_d, flush, stream)
+        line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sweeps = calibrate_sweeps(prob, args.cpu_seconds)
+        times, kind, asm = reference_cpu_path(prob, sweeps, 1, steps=1)
+        v = N * sweeps / 1e6 / times[0]
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                                "sample": f"{W}x{H}: hostLevinLaplacian ({asm:.2f} s) + {sweeps} gaussSeidel_host "
+                                          f"sweeps on 1 core (iterations are Gauss-Seidel sweeps)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
+    """Plain FP32 method: 25-band FP32 store + fused CG to 1e-6."""
+    import numpy as np
+    import torch
+
+    from gpumatting_b200 import api
+
+    W, H = prob.W, prob.H
+    N = W * H
+    a, b = api.levin_bands25(img_d, scr_d, eps=prob.eps, gamma_value=100.0, arithmetic="fp64")
+    Lm = api.DeviceBandedMatrix(a, torch.tensor(api.levin_band_offsets(W), device=a.device), N)
+    x = api.PaddedVector(N, api.levin_pad(W))
+    res_all, ms = [], []
+    for i in range(2 + args.plain_steps):
+        x.data.fill_(0.5)
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = api.banded_solve(Lm, x, b, W=W, solver="cg", rtol=1e-6, max_iters=5000, replace_every=50)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            res_all.append(r)
+            ms.append(e0.elapsed_time(e1))
+    it = statistics.mean(r.iters for r in res_all)
+    kms = statistics.mean(r.kernel_ms for r in res_all)
+    reps = statistics.mean(r.replacements for r in res_all)
+    alg = N * (it * KRYLOV_BYTES["ref25"] + reps * REPLACE_BYTES["ref25"] + IMPORT_BYTES["ref25"])
+    return {"ms_per_solve": statistics.mean(ms), "iters": it, "rel_residual": res_all[-1].rel_residual,
+            "mpix_iter_s": N * it / 1e6 / (statistics.mean(ms) / 1000), "kernel_ms": kms,
+            "achieved_gbs": alg / (kms / 1000) / 1e9, "status": res_all[-1].status}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--W", type=int, default=1920)
+    ap.add_argument("--H", type=int, default=1080)
+    ap.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,321 @@
+"""Python mirror of the reference's BandedMatrix / Vector / Solve API over
+libgpumat's C ABI.
+
+Device memory comes from torch (CUDA tensors); every computation runs in
+libgpumat.so.  Names follow the reference (main.cu, BandedMatrix.cu,
+Vector.cu, Matting.cu, Solve.cpp); the gm_* native layer adds the symmetric
+mixed-precision store, solver parameters and results.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream(stream=None) -> int:
+    torch = _torch()
+    s = torch.cuda.current_stream() if stream is None else stream
+    return s.cuda_stream
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def levin_band_offsets(W: int) -> np.ndarray:
+    """main.cu:164-190: offsets du + W dv at band 12 + du + 5 dv."""
+    o = (C.c_int * 25)()
+    L.load().gm_levin_band_offsets(W, o)
+    return np.array(list(o), np.int32)
+
+
+def levin_pad(W: int) -> int:
+    """main.cu:229."""
+    return int(L.load().gm_levin_pad(W))
+
+
+# ---------------------------------------------------------------------------
+# Reference data types
+# ---------------------------------------------------------------------------
+class DeviceBandedMatrix:
+    """A device BandedMatrix (BandedMatrix.h:23-38) backed by torch tensors.
+
+    ``a`` is (nbands, apitch) float32, band j of row i at a[j, i];
+    ``bands`` holds the int32 offsets on the device (as bmCopyToDevice leaves
+    them, BandedMatrix.cu:23-41).
+    """
+
+    def __init__(self, a, bands, rows: int):
+        torch = _torch()
+        assert a.dtype == torch.float32 and a.is_cuda and a.dim() == 2
+        self.a = a
+        self.bands = bands
+        self.rows = rows
+        self.nbands = a.shape[0]
+        self.apitch = a.stride(0)
+
+    @classmethod
+    def from_host(cls, a_host: np.ndarray, offsets, apitch: int | None = None, device="cuda"):
+        torch = _torch()
+        nb, rows = a_host.shape
+        ap = apitch or ((rows + 63) // 64) * 64
+        a = torch.zeros((nb, ap), dtype=torch.float32, device=device)
+        a[:, :rows] = torch.from_numpy(np.ascontiguousarray(a_host, np.float32)).to(device)
+        bands = torch.tensor(np.asarray(offsets, np.int32), dtype=torch.int32, device=device)
+        return cls(a, bands, rows)
+
+    @property
+    def struct(self) -> L.BandedMatrix:
+        return L.BandedMatrix(self.a.data_ptr(), self.apitch, self.bands.data_ptr(), self.nbands, self.rows,
+                              self.rows)
+
+
+class PaddedVector:
+    """Zero-padded device vector (Vector.cu:23-46): ``ptr`` is element 0."""
+
+    def __init__(self, n: int, pad: int, init=None, device="cuda"):
+        torch = _torch()
+        self.n, self.pad = n, pad
+        self.storage = torch.zeros(n + 2 * pad, dtype=torch.float32, device=device)
+        if init is not None:
+            self.storage[pad:pad + n] = torch.as_tensor(np.asarray(init, np.float32).ravel(), device=device)
+
+    @property
+    def ptr(self) -> int:
+        return self.storage.data_ptr() + 4 * self.pad
+
+    @property
+    def data(self):
+        return self.storage[self.pad:self.pad + self.n]
+
+
+# ---------------------------------------------------------------------------
+# Drop-in solvers (main.cu:406-556), device data, legacy stream
+# ---------------------------------------------------------------------------
+def cgSolve(alpha: PaddedVector, Lm: DeviceBandedMatrix, b, pad: int, iterations: int, restartInterval: int):
+    lib = L.load()
+    lib.cgSolve(alpha.ptr, Lm.struct, _ptr(b), pad, iterations, restartInterval)
+    L.check(lib.gm_last_status())
+
+
+def gradSolve(alpha: PaddedVector, Lm: DeviceBandedMatrix, b, iterations: int, pad: int):
+    lib = L.load()
+    lib.gradSolve(alpha.ptr, Lm.struct, _ptr(b), iterations, pad)
+    L.check(lib.gm_last_status())
+
+
+def jacobi(x: PaddedVector, a: DeviceBandedMatrix, b, omega: float, pad: int, iterations: int):
+    lib = L.load()
+    lib.jacobi(x.ptr, a.struct, _ptr(b), omega, pad, iterations)
+    L.check(lib.gm_last_status())
+
+
+def hostLevinLaplacian(bands_host: np.ndarray, b_host: np.ndarray, lam: float, im4: np.ndarray,
+                       scribs: np.ndarray, W: int, H: int, imPitch: int | None = None):
+    """Matting.cu:39-219 with host arrays; fills bands_host (25, N) and b_host."""
+    lib = L.load()
+    assert bands_host.dtype == np.float32 and bands_host.flags.c_contiguous and bands_host.shape[0] == 25
+    offs = levin_band_offsets(W)
+    m = L.BandedMatrix(bands_host.ctypes.data, bands_host.shape[1], offs.ctypes.data, 25, W * H, W * H)
+    im4 = np.ascontiguousarray(im4, np.float32)
+    sc = np.ascontiguousarray(scribs, np.uint8)
+    lib.hostLevinLaplacian(m, b_host.ctypes.data, lam, im4.ctypes.data, sc.ctypes.data, W, H, imPitch or W)
+    L.check(lib.gm_last_status())
+
+
+def jacobi_host(x_padded: np.ndarray, pad: int, bands_host: np.ndarray, offsets, b: np.ndarray, iterations: int,
+                omega: float = 2.0 / 3.0):
+    """Solve.cpp:35-85 semantics on host arrays (x_padded has `pad` zeros each side)."""
+    lib = L.load()
+    offs = np.ascontiguousarray(offsets, np.int32)
+    a = np.ascontiguousarray(bands_host, np.float32)
+    m = L.BandedMatrix(a.ctypes.data, a.shape[1], offs.ctypes.data, a.shape[0], a.shape[1], a.shape[1])
+    bb = np.ascontiguousarray(b, np.float32)
+    lib.jacobi_host(x_padded.ctypes.data + 4 * pad, C.byref(m), bb.ctypes.data, iterations, pad, omega)
+    L.check(lib.gm_last_status())
+
+
+def gaussSeidel_host(x_padded: np.ndarray, pad: int, bands_host: np.ndarray, offsets, b: np.ndarray,
+                     iterations: int):
+    lib = L.load()
+    offs = np.ascontiguousarray(offsets, np.int32)
+    a = np.ascontiguousarray(bands_host, np.float32)
+    m = L.BandedMatrix(a.ctypes.data, a.shape[1], offs.ctypes.data, a.shape[0], a.shape[1], a.shape[1])
+    bb = np.ascontiguousarray(b, np.float32)
+    lib.gaussSeidel_host(x_padded.ctypes.data + 4 * pad, C.byref(m), bb.ctypes.data, iterations)
+    L.check(lib.gm_last_status())
+
+
+# ---------------------------------------------------------------------------
+# L2 kernels
+# ---------------------------------------------------------------------------
+def bm_ax(b, Lm: DeviceBandedMatrix, x: PaddedVector, stream=None):
+    L.check(L.load().gm_bm_ax(_ptr(b), Lm.struct, x.ptr, _stream(stream)))
+
+
+def bm_axpy(b, Lm: DeviceBandedMatrix, x: PaddedVector, y, add: bool, stream=None):
+    L.check(L.load().gm_bm_axpy(_ptr(b), Lm.struct, x.ptr, _ptr(y), int(add), _stream(stream)))
+
+
+def jacobi_step(xx, x: PaddedVector, Lm: DeviceBandedMatrix, b, omega: float, stream=None):
+    L.check(L.load().gm_jacobi_step(_ptr(xx), x.ptr, Lm.struct, _ptr(b), omega, _stream(stream)))
+
+
+def inner_prod(x, y, stream=None, f64: bool = False):
+    torch = _torch()
+    out = torch.zeros(1, dtype=torch.float64 if f64 else torch.float32, device=x.device)
+    fn = L.load().gm_inner_prod_f64 if f64 else L.load().gm_inner_prod
+    L.check(fn(out.data_ptr(), x.data_ptr(), y.data_ptr(), x.numel(), _stream(stream)))
+    return out
+
+
+def compute_error(alpha, gt, W: int, H: int, stream=None) -> float:
+    v = C.c_double(0)
+    L.check(L.load().gm_compute_error(C.byref(v), alpha.data_ptr(), gt.data_ptr(), W, H, _stream(stream)))
+    return v.value
+
+
+# ---------------------------------------------------------------------------
+# Native: symmetric Levin store
+# ---------------------------------------------------------------------------
+PRECISIONS = {"fp32": L.GM_PREC_FP32, "fp16": L.GM_PREC_FP16, "bf16": L.GM_PREC_BF16}
+SOLVERS = {"cg": L.GM_SOLVER_CG, "gd": L.GM_SOLVER_GD, "jacobi": L.GM_SOLVER_JACOBI}
+
+
+def _image_desc(image) -> L.GmImage:
+    torch = _torch()
+    if image.dtype == torch.uint8:
+        assert image.dim() == 3 and image.shape[2] == 3 and image.is_contiguous()
+        return L.GmImage(image.data_ptr(), L.GM_IMAGE_RGB8, image.shape[1] * 3)
+    assert image.dtype == torch.float32 and image.dim() == 3 and image.shape[2] == 4 and image.is_contiguous()
+    return L.GmImage(image.data_ptr(), L.GM_IMAGE_RGBA32F, image.shape[1] * 16)
+
+
+def _scrib_desc(scribbles=None, gamma_value: float = 100.0, gamma_map=None, s_map=None) -> L.GmScribbles:
+    sc = L.GmScribbles()
+    sc.gamma_value = gamma_value
+    if scribbles is not None:
+        sc.map = scribbles.data_ptr()
+        sc.map_pitch = scribbles.shape[1]
+    if gamma_map is not None:
+        sc.gamma_map = gamma_map.data_ptr()
+        sc.s_map = None if s_map is None else s_map.data_ptr()
+    return sc
+
+
+@dataclass
+class SolveResult:
+    status: int
+    iters: int
+    replacements: int
+    rel_residual: float
+    kernel_ms: float
+    grid: int
+
+    @classmethod
+    def from_info(cls, info: L.GmSolveInfo) -> "SolveResult":
+        return cls(info.status, info.iters, info.replacements, info.rel_residual, info.kernel_ms, info.grid)
+
+
+class LevinStore:
+    """gm_levin_store: 12 planes of upper affinities (+ FP32 copy), gamma, b."""
+
+    def __init__(self, W: int, H: int, precision: str = "fp16"):
+        self.s = L.GmLevinStore()
+        L.check(L.load().gm_levin_store_alloc(C.byref(self.s), W, H, PRECISIONS[precision]))
+        self.W, self.H, self.precision = W, H, precision
+
+    def __del__(self):
+        try:
+            if self.s.owns:
+                L.load().gm_levin_store_free(C.byref(self.s))
+        except Exception:
+            pass
+
+    def assemble(self, image, scribbles=None, eps: float = 1e-5, gamma_value: float = 100.0, gamma_map=None,
+                 s_map=None, bands25: DeviceBandedMatrix | None = None, b25=None, stream=None):
+        im = _image_desc(image)
+        sc = _scrib_desc(scribbles, gamma_value, gamma_map, s_map)
+        bm = None if bands25 is None else C.byref(bands25.struct)
+        L.check(L.load().gm_levin_assemble(C.byref(self.s), C.byref(im), C.byref(sc), eps, bm, _ptr(b25),
+                                           _stream(stream)))
+        return self
+
+    def planes(self, which: str = "w32"):
+        """Views of the store's device planes as torch tensors (H, pitch)."""
+        torch = _torch()
+        W, H, P = self.W, self.H, self.s.pitch
+        n = H * P
+        if which == "w32":
+            return _wrap(self.s.w32, (12, H, P), torch.float32)
+        if which == "w":
+            dt = {"fp32": torch.float32, "fp16": torch.float16, "bf16": torch.bfloat16}[self.precision]
+            return _wrap(self.s.w, (12, H, P), dt)
+        if which == "gamma":
+            return _wrap(self.s.gamma, (H, P), torch.float32)
+        if which == "b":
+            return _wrap(self.s.b, (H, P), torch.float32)
+        raise KeyError(which)
+
+    def solve(self, alpha, solver: str = "cg", stream=None, **params) -> SolveResult:
+        p = L.default_params(solver=SOLVERS[solver], **params)
+        info = L.GmSolveInfo()
+        rc = L.load().gm_levin_solve(C.byref(self.s), alpha.data_ptr(), C.byref(p), C.byref(info), _stream(stream))
+        if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
+            L.check(rc)
+        return SolveResult.from_info(info)
+
+
+class _CudaArray:
+    """Minimal __cuda_array_interface__ holder so torch can view device
+    memory that libgpumat owns (no copy)."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _wrap(ptr: int, shape, dtype):
+    """Non-owning torch view of device memory owned by libgpumat."""
+    torch = _torch()
+    if dtype == torch.bfloat16:
+        return torch.as_tensor(_CudaArray(ptr, shape, "<i2"), device="cuda").view(torch.bfloat16)
+    ts = {torch.float32: "<f4", torch.float16: "<f2", torch.float64: "<f8"}[dtype]
+    return torch.as_tensor(_CudaArray(ptr, shape, ts), device="cuda")
+
+
+def levin_bands25(image, scribbles=None, eps: float = 1e-5, gamma_value: float = 100.0, gamma_map=None, s_map=None,
+                  arithmetic: str = "fp64", stream=None):
+    """25-band FP32 reference-layout store (a (25, N), b (N,)) on the device."""
+    torch = _torch()
+    H, W = image.shape[0], image.shape[1]
+    N = W * H
+    a = torch.empty((25, N), dtype=torch.float32, device=image.device)
+    b = torch.empty(N, dtype=torch.float32, device=image.device)
+    im = _image_desc(image)
+    sc = _scrib_desc(scribbles, gamma_value, gamma_map, s_map)
+    ar = L.GM_ASSEMBLY_REFERENCE if arithmetic == "reference" else L.GM_ASSEMBLY_FP64
+    L.check(L.load().gm_levin_assemble_bands25(a.data_ptr(), N, b.data_ptr(), C.byref(im), C.byref(sc), eps, W, H,
+                                               ar, _stream(stream)))
+    return a, b
+
+
+def banded_solve(Lm: DeviceBandedMatrix, alpha: PaddedVector, b, W: int = 0, solver: str = "cg", stream=None,
+                 **params) -> SolveResult:
+    p = L.default_params(solver=SOLVERS[solver], **params)
+    info = L.GmSolveInfo()
+    rc = L.load().gm_banded_solve(Lm.struct, W, alpha.ptr, alpha.pad, _ptr(b), C.byref(p), C.byref(info),
+                                  _stream(stream))
+    if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
+        L.check(rc)
+    return SolveResult.from_info(info)

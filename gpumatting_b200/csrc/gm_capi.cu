@@ -1,0 +1,346 @@
+// gm_capi.cu -- C-ABI front ends: the native solve entry points and the
+// reference-named drop-ins (main.cu, Matting.cu, Solve.cpp).
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gm_solver_api.h"
+
+int gm_note_status(int s);
+
+namespace gm {
+int generic_solve(const BandedMatrix& L, float* alpha, int pad, const float* b, const gm_solve_params& p,
+                  gm_solve_info* info, cudaStream_t st);
+
+// True when offs is the 25-band Levin stencil of an image W wide
+// (main.cu:164-190) and rows is a whole number of image rows.
+static bool levin_pattern(const int* offs, int nb, int rows, int* W_out)
+{
+    if (nb != 25) return false;
+    const int W = offs[17];  // band 12 + 5: offset W
+    if (W < 1 || rows % W != 0) return false;
+    for (int dv = -2; dv <= 2; ++dv)
+        for (int du = -2; du <= 2; ++du)
+            if (offs[12 + du + 5 * dv] != du + W * dv) return false;
+    *W_out = W;
+    return true;
+}
+
+// 9-colour Gauss-Seidel sweep on the Levin stencil: pixels with
+// (u mod 3, v mod 3) == colour never neighbour each other in the 5x5
+// stencil, so one colour updates in parallel with the same arithmetic as
+// Solve.cpp:16-31 (middle band skipped, then divided by it).
+__global__ void gs_colour_kernel(float* x, const float* __restrict__ a, size_t apitch, const int* __restrict__ bands,
+                                 int nbands, int W, int H, const float* __restrict__ b, int cu, int cv)
+{
+    __shared__ int off[32];
+    for (int j = threadIdx.x; j < nbands; j += blockDim.x) off[j] = bands[j];
+    __syncthreads();
+    const int nu = (W - cu + 2) / 3, nv = (H - cv + 2) / 3;
+    const int mid = nbands / 2;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nu * nv; t += gridDim.x * blockDim.x) {
+        const int u = cu + 3 * (t % nu), v = cv + 3 * (t / nu);
+        const size_t i = (size_t)v * W + u;
+        float s = 0.f;
+        for (int j = 0; j < nbands; ++j) {
+            if (j == mid) continue;
+            s += a[i + (size_t)j * apitch] * x[(long long)i + off[j]];
+        }
+        x[i] = (b[i] - s) / a[i + (size_t)mid * apitch];
+    }
+}
+
+}  // namespace gm
+
+using namespace gm;
+
+static int read_offsets(const BandedMatrix& L, std::vector<int>& offs, cudaStream_t st)
+{
+    offs.resize(L.nbands > 0 ? L.nbands : 0);
+    if (L.nbands <= 0 || !L.bands) { gm_set_error_msg("matrix has no bands"); return GM_ERR_INVALID; }
+    GM_CUDA_TRY(cudaMemcpyAsync(offs.data(), L.bands, sizeof(int) * L.nbands, cudaMemcpyDeviceToHost, st));
+    GM_CUDA_TRY(cudaStreamSynchronize(st));
+    return GM_OK;
+}
+
+extern "C" int gm_banded_solve(BandedMatrix L, int W, float* alpha, int pad, const float* b,
+                               const gm_solve_params* prm, gm_solve_info* info, void* stream)
+{
+    gm_solve_params p;
+    if (prm) p = *prm; else gm_default_params(&p);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!alpha || !b || !L.a || L.rows <= 0) { gm_set_error_msg("gm_banded_solve: bad arguments"); return GM_ERR_INVALID; }
+    std::vector<int> offs;
+    GM_TRY(read_offsets(L, offs, st));
+    int Wd = 0;
+    const bool lev = levin_pattern(offs.data(), L.nbands, L.rows, &Wd) && (W <= 0 || W == Wd);
+    if (!lev) {
+        if (W > 0) { gm_set_error_msg("band offsets are not the Levin stencil of width %d", W); return GM_ERR_INVALID; }
+        return generic_solve(L, alpha, pad, b, p, info, st);
+    }
+    W = Wd;
+    const int H = L.rows / W;
+    const int P = (W + 7) & ~7;
+    SolverSetup S;
+    memset(&S, 0, sizeof(S));
+    S.W = W;
+    S.H = H;
+    float* tmp = nullptr;
+    const float* planes = L.a;
+    uint64_t rs = (uint64_t)W * 4, ps = (uint64_t)L.apitch * 4;
+    if (W % 4 != 0 || L.apitch % 4 != 0 || ((uintptr_t)L.a & 15)) {
+        // Repack into a pitched copy that tensor maps can address.
+        GM_CUDA_TRY(cudaMallocAsync((void**)&tmp, (size_t)25 * H * P * 4, st));
+        for (int k = 0; k < 25; ++k)
+            GM_CUDA_TRY(cudaMemcpy2DAsync(tmp + (size_t)k * H * P, (size_t)P * 4, L.a + (size_t)k * L.apitch,
+                                          (size_t)W * 4, (size_t)W * 4, H, cudaMemcpyDeviceToDevice, st));
+        planes = tmp;
+        rs = (uint64_t)P * 4;
+        ps = (uint64_t)H * P * 4;
+    }
+    OpSource op;
+    op.kind = OP_REF25;
+    op.dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    op.esize = 4;
+    op.base = planes;
+    op.row_stride = rs;
+    op.plane_stride = ps;
+    op.planes = 25;
+    S.lo = op;
+    S.hi = op;
+    S.mixed = false;
+    S.b = b;
+    S.bpitch = W;
+    S.alpha_in = alpha;
+    S.alpha_out = alpha;
+    S.alpha_pitch = W;
+    int rc = run_solver(S, &p, info, st);
+    if (tmp) cudaFreeAsync(tmp, st);
+    return rc;
+}
+
+extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const gm_solve_params* prm,
+                              gm_solve_info* info, void* stream)
+{
+    gm_solve_params p;
+    if (prm) p = *prm; else gm_default_params(&p);
+    if (!store || !store->w32 || !alpha) { gm_set_error_msg("gm_levin_solve: bad arguments"); return GM_ERR_INVALID; }
+    const int W = store->W, H = store->H, P = store->pitch;
+    SolverSetup S;
+    memset(&S, 0, sizeof(S));
+    S.W = W;
+    S.H = H;
+    OpSource hi;
+    hi.kind = OP_SYM;
+    hi.dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    hi.esize = 4;
+    hi.base = store->w32;
+    hi.row_stride = (uint64_t)P * 4;
+    hi.plane_stride = (uint64_t)H * P * 4;
+    hi.planes = 12;
+    OpSource lo = hi;
+    if (p.use_low && store->precision != GM_PREC_FP32) {
+        lo.dt = store->precision == GM_PREC_FP16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+        lo.esize = 2;
+        lo.base = store->w;
+        lo.row_stride = (uint64_t)P * 2;
+        lo.plane_stride = (uint64_t)H * P * 2;
+    }
+    S.lo = lo;
+    S.hi = hi;
+    S.mixed = true;
+    S.gamma = store->gamma;
+    S.gamma_pitch = P;
+    S.b = store->b;
+    S.bpitch = P;
+    S.alpha_in = alpha;
+    S.alpha_out = alpha;
+    S.alpha_pitch = W;
+    return run_solver(S, &p, info, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Drop-ins
+// ---------------------------------------------------------------------------
+
+// main.cu:458-526
+extern "C" void cgSolve(float* alpha, BandedMatrix L, float* b, int pad, int iterations, int restartInterval)
+{
+    gm_solve_params p;
+    gm_default_params(&p);
+    p.solver = GM_SOLVER_CG;
+    p.rtol = 0.0;
+    p.max_iters = iterations > 0 ? iterations : 0;
+    p.restart = restartInterval > 0 ? restartInterval : 0;
+    p.replace_every = 0;
+    gm_solve_info info;
+    gm_note_status(gm_banded_solve(L, 0, alpha, pad, b, &p, &info, nullptr));
+}
+
+// main.cu:406-456: the reference recomputes d = L alpha - b every iteration,
+// so the drop-in replaces the residual every iteration too.
+extern "C" void gradSolve(float* alpha, BandedMatrix L, float* b, int iterations, int pad)
+{
+    gm_solve_params p;
+    gm_default_params(&p);
+    p.solver = GM_SOLVER_GD;
+    p.rtol = 0.0;
+    p.max_iters = iterations > 0 ? iterations : 0;
+    p.replace_every = 1;
+    gm_solve_info info;
+    gm_note_status(gm_banded_solve(L, 0, alpha, pad, b, &p, &info, nullptr));
+}
+
+// main.cu:528-556.  The reference swaps x and its scratch buffer each sweep,
+// so after an odd count its last iterate sits in the freed scratch; here the
+// last iterate is always returned in x.
+extern "C" void jacobi(float* x, const BandedMatrix a, const float* b, float omega, int pad, int iterations)
+{
+    gm_solve_params p;
+    gm_default_params(&p);
+    p.solver = GM_SOLVER_JACOBI;
+    p.rtol = 0.0;
+    p.max_iters = iterations > 0 ? iterations : 0;
+    p.omega = omega;
+    gm_solve_info info;
+    gm_note_status(gm_banded_solve(a, 0, x, pad, b, &p, &info, nullptr));
+}
+
+// Matting.cu:39-219 on the GPU with the reference's arithmetic.  The
+// reference accumulates into a zeroed L.a; this writes the final values.
+extern "C" void hostLevinLaplacian(BandedMatrix L, float* b, float lambda, gm_float4* im, unsigned char* scribs,
+                                   int imW, int imH, size_t imPitch)
+{
+    if (!L.a || !b || !im || !scribs || imW <= 0 || imH <= 0 || imPitch < (size_t)imW || L.nbands != 25 ||
+        L.rows != imW * imH || L.apitch < (size_t)L.rows) {
+        gm_set_error_msg("hostLevinLaplacian: bad arguments (need 25 bands, rows = W*H)");
+        gm_note_status(GM_ERR_INVALID);
+        return;
+    }
+    const size_t N = (size_t)imW * imH;
+    float4* dim = nullptr;
+    unsigned char* dsc = nullptr;
+    float* da = nullptr;
+    float* db = nullptr;
+    int rc = GM_OK;
+    if (cudaMalloc((void**)&dim, imPitch * imH * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc((void**)&dsc, imPitch * imH) != cudaSuccess ||
+        cudaMalloc((void**)&da, 25 * N * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&db, N * sizeof(float)) != cudaSuccess)
+        rc = GM_ERR_NOMEM;
+    if (rc == GM_OK && (cudaMemcpy(dim, im, imPitch * imH * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(dsc, scribs, imPitch * imH, cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = GM_ERR_CUDA;
+    if (rc == GM_OK) {
+        gm_image gi;
+        gi.data = dim;
+        gi.format = GM_IMAGE_RGBA32F;
+        gi.pitch_bytes = imPitch * sizeof(float4);
+        gm_scribbles sc;
+        memset(&sc, 0, sizeof(sc));
+        sc.map = dsc;
+        sc.map_pitch = imPitch;
+        sc.gamma_value = 1.0f;  // Matting.cu:48
+        rc = gm_levin_assemble_bands25(da, N, db, &gi, &sc, lambda, imW, imH, GM_ASSEMBLY_REFERENCE, nullptr);
+    }
+    if (rc == GM_OK &&
+        (cudaMemcpy2D(L.a, L.apitch * sizeof(float), da, N * sizeof(float), N * sizeof(float), 25,
+                      cudaMemcpyDeviceToHost) != cudaSuccess ||
+         cudaMemcpy(b, db, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess))
+        rc = GM_ERR_CUDA;
+    cudaFree(dim);
+    cudaFree(dsc);
+    cudaFree(da);
+    cudaFree(db);
+    gm_note_status(rc);
+}
+
+// Host BandedMatrix -> device copy helper for the *_host drop-ins.
+static int host_to_device(const BandedMatrix* A, BandedMatrix* dA)
+{
+    bmCopyToDevice(dA, A);
+    return gm_last_status();
+}
+
+// Solve.cpp:35-85 on the GPU.  The reference's diagonal is band nbands/2;
+// the Levin store (and every pattern this accepts) keeps offset 0 there.
+extern "C" void jacobi_host(float* x, const BandedMatrix* A, const float* b, size_t iterations, int xpad,
+                            float omega)
+{
+    if (!x || !A || !b || xpad < 0) { gm_set_error_msg("jacobi_host: bad arguments"); gm_note_status(GM_ERR_INVALID); return; }
+    const int n = A->rows;
+    if (A->nbands <= 0 || A->bands[A->nbands / 2] != 0) {
+        gm_set_error_msg("jacobi_host: the middle band must be the diagonal");
+        gm_note_status(GM_ERR_INVALID);
+        return;
+    }
+    BandedMatrix dA;
+    int rc = host_to_device(A, &dA);
+    float* dx = nullptr;
+    float* dbv = nullptr;
+    if (rc == GM_OK) {
+        vecDeviceMalloc(&dx, n, xpad, xpad);
+        rc = gm_last_status();
+    }
+    if (rc == GM_OK && (cudaMalloc((void**)&dbv, sizeof(float) * (n > 0 ? n : 1)) != cudaSuccess)) rc = GM_ERR_NOMEM;
+    if (rc == GM_OK && (cudaMemcpy(dx, x, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(dbv, b, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = GM_ERR_CUDA;
+    if (rc == GM_OK) {
+        gm_solve_params p;
+        gm_default_params(&p);
+        p.solver = GM_SOLVER_JACOBI;
+        p.rtol = 0.0;
+        p.max_iters = (int)iterations;
+        p.omega = omega;
+        gm_solve_info info;
+        rc = gm_banded_solve(dA, 0, dx, xpad, dbv, &p, &info, nullptr);
+        if (rc == GM_OK && cudaMemcpy(x, dx, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) rc = GM_ERR_CUDA;
+    }
+    if (dx) vecDeviceFree(dx, xpad);
+    if (dbv) cudaFree(dbv);
+    bmDeviceFree(&dA);
+    gm_note_status(rc);
+}
+
+// Solve.cpp:3-33 on the GPU as 9-colour Gauss-Seidel (Levin stencil only).
+extern "C" void gaussSeidel_host(float* x, const BandedMatrix* A, const float* b, size_t iterations)
+{
+    if (!x || !A || !b) { gm_set_error_msg("gaussSeidel_host: bad arguments"); gm_note_status(GM_ERR_INVALID); return; }
+    int W = 0;
+    if (!levin_pattern(A->bands, A->nbands, A->rows, &W)) {
+        gm_set_error_msg("gaussSeidel_host: only the 25-band Levin stencil is supported");
+        gm_note_status(GM_ERR_UNSUPPORTED);
+        return;
+    }
+    const int n = A->rows, H = n / W;
+    const int pad = 2 * W + 2;
+    BandedMatrix dA;
+    int rc = host_to_device(A, &dA);
+    float* dx = nullptr;
+    float* dbv = nullptr;
+    if (rc == GM_OK) {
+        vecDeviceMalloc(&dx, n, pad, pad);
+        rc = gm_last_status();
+    }
+    if (rc == GM_OK && cudaMalloc((void**)&dbv, sizeof(float) * n) != cudaSuccess) rc = GM_ERR_NOMEM;
+    if (rc == GM_OK && (cudaMemcpy(dx, x, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(dbv, b, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = GM_ERR_CUDA;
+    if (rc == GM_OK) {
+        for (size_t it = 0; it < iterations; ++it)
+            for (int c = 0; c < 9; ++c) {
+                const int cu = c % 3, cv = c / 3;
+                const int cnt = ((W - cu + 2) / 3) * ((H - cv + 2) / 3);
+                const int nb = std::max(1, std::min((cnt + 255) / 256, 148 * 4));
+                gs_colour_kernel<<<nb, 256>>>(dx, dA.a, dA.apitch, dA.bands, 25, W, H, dbv, cu, cv);
+            }
+        if (cudaGetLastError() != cudaSuccess) rc = GM_ERR_CUDA;
+        if (rc == GM_OK && cudaMemcpy(x, dx, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) rc = GM_ERR_CUDA;
+    }
+    if (dx) vecDeviceFree(dx, pad);
+    if (dbv) cudaFree(dbv);
+    bmDeviceFree(&dA);
+    gm_note_status(rc);
+}

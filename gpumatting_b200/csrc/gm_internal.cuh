@@ -1,0 +1,275 @@
+// gm_internal.cuh -- shared device and host helpers of libgpumat.
+//
+// Device side: TMA (cp.async.bulk.tensor) row loads completed on mbarriers,
+// a grid barrier with a wall-clock limit, and deterministic FP64 block
+// reductions.  Host side: status plumbing and tensor-map encoding through the
+// driver entry point (no libcuda link needed).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/gpumat.h"
+
+#define GM_CUDA_TRY(expr)                                                     \
+    do {                                                                      \
+        cudaError_t _e = (expr);                                              \
+        if (_e != cudaSuccess) {                                              \
+            gm_set_error_msg("%s:%d: %s: %s", __FILE__, __LINE__, #expr,      \
+                             cudaGetErrorString(_e));                         \
+            return GM_ERR_CUDA;                                               \
+        }                                                                     \
+    } while (0)
+
+#define GM_TRY(expr)                                                          \
+    do {                                                                      \
+        int _s = (expr);                                                      \
+        if (_s != GM_OK) return _s;                                           \
+    } while (0)
+
+// Records a message for gm_last_error() (thread-local).
+void gm_set_error_msg(const char* fmt, ...);
+
+// Checks that the current device is sm_100 class; returns GM_ERR_UNSUPPORTED
+// otherwise.
+int gm_check_device(int* sm_count);
+
+// ---------------------------------------------------------------------------
+// Tensor maps
+// ---------------------------------------------------------------------------
+
+// Encodes a tiled tensor map of rank 2 or 3 (dims innermost first, strides
+// in bytes for dims 1..rank-1) with zero out-of-bounds fill and no swizzle.
+int gm_make_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int rank, void* base,
+                 const uint64_t* dims, const uint64_t* strides_bytes,
+                 const uint32_t* box);
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+namespace gm {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t* bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Orders this thread's earlier generic-proxy accesses (shared and global)
+// before its later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map)
+{
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ int ld_volatile_int(const int* p)
+{
+    return *reinterpret_cast<const volatile int*>(p);
+}
+
+// Grid barrier state, zeroed before the launch.  `abort` carries the first
+// error any CTA raised (GM_ERR_TIMEOUT from a wait that hit its limit, or a
+// solver status); every wait also returns once it is set.
+struct GridBarrier {
+    unsigned count;
+    unsigned gen;
+    int abort;
+    int where;  // which wait gave up: 1 = grid barrier, 2 = TMA row wait
+};
+
+// All CTAs of the grid call this the same number of times.  Returns false
+// when the barrier was abandoned (limit reached or abort set by any CTA).
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, uint64_t limit_ns)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned g = ld_acquire(&gb->gen);
+        __threadfence();
+        unsigned arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == nblocks - 1) {
+            gb->count = 0;
+            __threadfence();
+            st_release(&gb->gen, g + 1);
+        } else {
+            uint64_t t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (ld_acquire(&gb->gen) == g) {
+                if (ld_volatile_int(&gb->abort)) { ok = 0; break; }
+                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
+                    atomicExch(&gb->where, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+        if (ld_volatile_int(&gb->abort)) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Waits for the mbarrier phase with a wall-clock limit; on expiry raises
+// GM_ERR_TIMEOUT in the grid barrier state and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, GridBarrier* gb,
+                                                  uint64_t limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    uint64_t t0 = globaltimer_ns();
+    unsigned spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) {
+            atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
+            atomicExch(&gb->where, 2);
+            return false;
+        }
+    }
+    return true;
+}
+
+// Deterministic block sum of NV doubles: fixed shuffle tree per warp, then
+// warp 0 adds the warp sums in warp order.  Result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch /* >= 32*NV */)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) scratch[wid * NV + k] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? scratch[lane * NV + k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            v[k] = x;
+        }
+    }
+    __syncthreads();
+}
+
+// Sums partials[0..n) (stride NV, component k) in a fixed order using warp
+// 0 of the calling block; every CTA that calls this with the same data gets
+// bit-identical results.  Reads bypass L1 (other CTAs wrote the data).
+template <int NV>
+__device__ __forceinline__ void grid_total(const double* partials, int n, double (&out)[NV], double* bcast)
+{
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = 0.0;
+            for (int i = lane; i < n; i += 32) x += __ldcg(partials + (size_t)i * NV + k);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) bcast[k] = x;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = bcast[k];
+    __syncthreads();
+}
+
+template <class T> struct Cvt;
+template <> struct Cvt<float> {
+    static __device__ __forceinline__ float to_f(float x) { return x; }
+};
+template <> struct Cvt<__half> {
+    static __device__ __forceinline__ float to_f(__half x) { return __half2float(x); }
+};
+template <> struct Cvt<__nv_bfloat16> {
+    static __device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
+};
+
+}  // namespace gm

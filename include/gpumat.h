@@ -1,0 +1,250 @@
+/* gpumat.h -- C ABI of libgpumat, the B200 (sm_100a) closed-form matting
+ * hot path.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the reference's names, arguments and
+ *     semantics (void returns, legacy default stream, caller-owned memory):
+ *     the BandedMatrix / Vector / Solve API of gpumatting.  Each cites the
+ *     reference function it replaces (paths within the gpumatting tree).
+ *     Errors are reported through gm_last_status() / gm_last_error().
+ *
+ *  2. The native gm_* API: status returns, an explicit cudaStream_t
+ *     (passed as void*), solver parameters and results, the symmetric
+ *     mixed-precision band store, the adjoint and batched solves.
+ *
+ * Memory layout conventions
+ *   - A BandedMatrix holds nbands planes of `rows` floats, band j of row i at
+ *     a[i + j*apitch]; bands[j] is the column offset (BandedMatrix.h:23-38).
+ *     On the device, apitch is in floats (BandedMatrix.cu:39).
+ *   - Reference vectors are zero-padded on both sides and the pointer points
+ *     at element 0 (Vector.cu:23-30); the Levin store needs a pad of at least
+ *     2W+2 (main.cu:229 uses ((2W+2)/32)*32+32).
+ *   - gm_levin_store planes are row-major [H][pitch] with pitch a multiple
+ *     of 8 elements >= W.
+ * All device pointers must be 16-byte aligned unless stated otherwise.
+ */
+#ifndef GPUMAT_H
+#define GPUMAT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status                                                              */
+/* ------------------------------------------------------------------ */
+enum {
+    GM_OK = 0,
+    GM_ERR_INVALID = 1,        /* bad argument (sizes, alignment, nulls)      */
+    GM_ERR_CUDA = 2,           /* a CUDA runtime call failed                  */
+    GM_ERR_UNSUPPORTED = 3,    /* device is not sm_100 class, or shape unsupported */
+    GM_ERR_TIMEOUT = 4,        /* a bounded wait inside a kernel gave up      */
+    GM_ERR_BREAKDOWN = 5,      /* p^T A p <= 0 or a non-finite scalar         */
+    GM_ERR_NOT_CONVERGED = 6,  /* max_iters reached above rtol                */
+    GM_ERR_NOMEM = 7           /* device allocation failed                    */
+};
+
+int gm_last_status(void);
+const char* gm_last_error(void);
+const char* gm_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Reference-compatible types and drop-in entry points                 */
+/* ------------------------------------------------------------------ */
+
+/* BandedMatrix.h:23-38 (same field order and types). */
+typedef struct BandedMatrix_s {
+    float* a;
+    size_t apitch;
+    int* bands;
+    int nbands;
+    int rows;
+    int cols;
+} BandedMatrix;
+
+/* float4 of the reference's RGBA images (ppm.h:309-333). */
+typedef struct gm_float4_s { float x, y, z, w; } gm_float4;
+
+/* BandedMatrix.cu:23-41: allocate a pitched device copy of a host matrix;
+ * dA->apitch is returned in floats. */
+void bmCopyToDevice(BandedMatrix* dA, const BandedMatrix* hA);
+/* BandedMatrix.cu:43-47 */
+void bmDeviceFree(BandedMatrix* dA);
+/* Vector.cu:23-30: zeroed device vector of length+lpad+rpad floats; *dx
+ * points at element 0 (after the left pad). */
+void vecDeviceMalloc(float** dx, int length, int leftPadding, int rightPadding);
+/* Vector.cu:37-41 */
+void vecCopyToDevice(float** dx, const float* hx, int length, int leftPadding, int rightPadding);
+/* Vector.cu:43-46 */
+void vecDeviceFree(float* dx, int leftPadding);
+
+/* main.cu:57 / :458-526: `iterations` CG iterations on L alpha = b (device
+ * data, alpha padded by `pad`), restarting every restartInterval. */
+void cgSolve(float* alpha, BandedMatrix L, float* b, int pad, int iterations, int restartInterval);
+/* main.cu:46 / :406-456: steepest descent with exact line search. */
+void gradSolve(float* alpha, BandedMatrix L, float* b, int iterations, int pad);
+/* main.cu:77-84 / :528-556: damped Jacobi sweeps (result left in x). */
+void jacobi(float* x, const BandedMatrix a, const float* b, float omega, int pad, int iterations);
+
+/* Matting.cu:39-219: Levin Laplacian + scribbles into the 25-band store.
+ * HOST pointers, as in the reference; the work runs on the GPU with the
+ * reference's arithmetic (results bit-identical) and gamma = 1. */
+void hostLevinLaplacian(BandedMatrix L, float* b, float lambda, gm_float4* im,
+                        unsigned char* scribs, int imW, int imH, size_t imPitch);
+
+/* Solve.cpp:3-33 / Solve.h:17.  HOST vectors.  Runs on the GPU as a
+ * multi-colour (9 colours over the 5x5 stencil) Gauss-Seidel sweep: same
+ * fixed point as the sequential sweep, different visiting order. */
+void gaussSeidel_host(float* x, const BandedMatrix* A, const float* b, size_t iterations);
+/* Solve.cpp:35-85 / Solve.h:31.  HOST vectors (x padded by xpad); runs the
+ * damped Jacobi iteration on the GPU and returns the last iterate in x. */
+void jacobi_host(float* x, const BandedMatrix* A, const float* b, size_t iterations, int xpad,
+                 float omega);
+
+/* main.cu:558-577: prints "Ground truth MSE: %.3e" for HOST alpha/gt. */
+void computeError(float* alpha, float* gtAlpha, int imW, int imH);
+
+/* ------------------------------------------------------------------ */
+/* Native API: kernels of the reference's L2 layer                     */
+/* stream arguments are cudaStream_t passed as void* (NULL = legacy).  */
+/* ------------------------------------------------------------------ */
+
+/* b = A x (BandedMatrix.cu:107-141, :194-198); x padded so x[i+bands[j]]
+ * is addressable for every row; a and b on the device. */
+int gm_bm_ax(float* b, BandedMatrix a, const float* x, void* stream);
+/* b = A x + y (add != 0) or A x - y (BandedMatrix.cu:152-189, :203-207). */
+int gm_bm_axpy(float* b, BandedMatrix a, const float* x, const float* y, int add, void* stream);
+/* xx = omega (x + (b - A x) / a_ii) + (1 - omega) x (BandedMatrix.cu:61-98);
+ * the diagonal is the band with offset 0. */
+int gm_jacobi_step(float* xx, const float* x, BandedMatrix a, const float* b, float omega,
+                   void* stream);
+/* *result = <x, y> in FP64 with a fixed summation order, rounded to float
+ * (Vector.cu:195-265, without its inter-block race). result on the device. */
+int gm_inner_prod(float* result, const float* x, const float* y, int len, void* stream);
+/* FP64 result, written to a device double. */
+int gm_inner_prod_f64(double* result, const float* x, const float* y, int len, void* stream);
+/* Vector.cu:124-183 */
+int gm_vec_add(float* result, const float* x, const float* y, int len, void* stream);
+int gm_vec_sub(float* result, const float* x, const float* y, int len, void* stream);
+int gm_vec_scale_const(float* result, const float* x, float s, int len, void* stream);
+/* s is a device scalar (vecScale_k). */
+int gm_vec_scale(float* result, const float* x, const float* s, int len, void* stream);
+
+/* 25 offsets of the Levin stencil, centre at index 12 (main.cu:164-190). */
+void gm_levin_band_offsets(int W, int offs[25]);
+/* main.cu:229: ((2W+2)/32)*32+32. */
+int gm_levin_pad(int W);
+
+/* Clamped MSE (main.cu:558-577), FP64 accumulation; device inputs. */
+int gm_compute_error(double* mse_host, const float* alpha, const float* gt, int W, int H,
+                     void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Native API: Levin store, assembly and solvers                       */
+/* ------------------------------------------------------------------ */
+
+enum { GM_PREC_FP32 = 0, GM_PREC_FP16 = 1, GM_PREC_BF16 = 2 };
+enum { GM_SOLVER_CG = 0, GM_SOLVER_GD = 1, GM_SOLVER_JACOBI = 2 };
+enum { GM_IMAGE_RGB8 = 0, GM_IMAGE_RGBA32F = 1 };
+/* Assembly arithmetic: FP64 throughout (rounded once), or the reference's
+ * float/double mix (bit-identical to hostLevinLaplacian). */
+enum { GM_ASSEMBLY_FP64 = 0, GM_ASSEMBLY_REFERENCE = 1 };
+
+typedef struct gm_image_s {
+    const void* data;     /* device pointer                               */
+    int format;           /* GM_IMAGE_RGB8 (3 bytes/px) or GM_IMAGE_RGBA32F */
+    size_t pitch_bytes;   /* bytes between image rows                     */
+} gm_image;
+
+/* Scribbles: either a uint8 map (0 background, 255 foreground, anything
+ * else unknown; Matting.cu:205-216) with one weight gamma_value, or per-pixel
+ * weights gamma_map and targets s_map ([H][W] floats).  Device pointers. */
+typedef struct gm_scribbles_s {
+    const uint8_t* map;
+    size_t map_pitch;     /* bytes between rows of map                     */
+    float gamma_value;
+    const float* gamma_map;
+    const float* s_map;
+} gm_scribbles;
+
+/* Symmetric Levin store: 12 planes of upper affinities
+ * w_k(i) = -L(i, i + du_k + W dv_k), k = du + 5 dv in 1..12, the diagonal
+ * being implicit (sum of the row's affinities, so rows of L sum to zero
+ * exactly) plus gamma_i.  All planes are [H][pitch] on the device. */
+typedef struct gm_levin_store_s {
+    int W, H, pitch;
+    int precision;        /* element type of w                            */
+    void* w;              /* [12][H][pitch] affinities in `precision`     */
+    float* w32;           /* [12][H][pitch] FP32 affinities (true operator) */
+    float* gamma;         /* [H][pitch] scribble weight                   */
+    float* b;             /* [H][pitch] right-hand side gamma_i * s_i      */
+    int owns;             /* set by gm_levin_store_alloc                  */
+} gm_levin_store;
+
+int gm_levin_store_alloc(gm_levin_store* st, int W, int H, int precision);
+int gm_levin_store_free(gm_levin_store* st);
+
+/* Assemble the symmetric store (FP64 arithmetic, rounded once) from an
+ * image and scribbles (Matting.cu:79-218 math with eps and gamma as
+ * parameters).  If bands25 is not NULL it also receives the reference's
+ * 25-band FP32 layout: nbands=25, apitch floats, offsets gm_levin_band_offsets,
+ * rows = W*H; bands25->a must be device memory of 25*apitch floats. */
+int gm_levin_assemble(gm_levin_store* st, const gm_image* im, const gm_scribbles* sc,
+                      double eps, BandedMatrix* bands25, float* b25, void* stream);
+
+/* Reference-layout assembly only (25 bands FP32 + b), with either
+ * arithmetic.  a, b: device; a has 25 planes of apitch floats. */
+int gm_levin_assemble_bands25(float* a, size_t apitch, float* b, const gm_image* im,
+                              const gm_scribbles* sc, double eps, int W, int H, int arithmetic,
+                              void* stream);
+
+typedef struct gm_solve_params_s {
+    int solver;           /* GM_SOLVER_*                                   */
+    double rtol;          /* stop at ||b - A x|| <= rtol ||b||; <= 0: run max_iters */
+    int max_iters;
+    int restart;          /* CG: reset the search direction every `restart` iterations (0 = never) */
+    int replace_every;    /* true-residual replacement period (0 = only at exit) */
+    float omega;          /* Jacobi damping                                */
+    int use_low;          /* mixed store: 1 = iterate with the low-precision planes */
+    double timeout_s;     /* limit on any single wait inside the kernel     */
+    int ctas_per_sm;      /* 0 = auto                                      */
+    int strip_width;      /* columns per CTA strip, multiple of 8, <= 240 (0 = auto) */
+    int inject;           /* test hook, 0 in normal use: 1 = the first grid barrier
+                             waits for one arrival that never comes, so the call
+                             must end with GM_ERR_TIMEOUT after timeout_s */
+} gm_solve_params;
+
+typedef struct gm_solve_info_s {
+    int status;
+    int iters;            /* Krylov (or Jacobi) sweeps applied to x        */
+    int replacements;     /* true-residual sweeps run                      */
+    double rel_residual;  /* ||b - A x|| / ||b|| of the returned x, FP64, true operator */
+    double bnorm;
+    float kernel_ms;      /* device time of the solver kernel              */
+    int grid;             /* CTAs launched                                  */
+    int where;            /* which bounded wait gave up, if any            */
+} gm_solve_info;
+
+void gm_default_params(gm_solve_params* p);
+
+/* Solve (L + diag(gamma)) alpha = b with the store's operator.  alpha:
+ * device [H][W] floats (pitch W), initial guess in, solution out. */
+int gm_levin_solve(const gm_levin_store* st, float* alpha, const gm_solve_params* p,
+                   gm_solve_info* info, void* stream);
+
+/* Solve with a 25-band BandedMatrix on the device (reference layout).
+ * W > 0 declares the Levin stencil of an image W wide (rows = W*H) and
+ * selects the fused stencil kernel; W = 0 (or offsets that are not the Levin
+ * pattern) uses the generic band path.  alpha padded as in the reference
+ * (pad >= max |offset|), b unpadded, both device. */
+int gm_banded_solve(BandedMatrix L, int W, float* alpha, int pad, const float* b,
+                    const gm_solve_params* p, gm_solve_info* info, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUMAT_H */

@@ -1,0 +1,67 @@
+/* ref_shim.cu -- C entry points onto the reference's own CPU code.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Compiled by oracle/Makefile from the reference
+ * sources where they lie (the reference tree is put on the include path);
+ * nothing of the reference is copied here.  Output goes to oracle/_ref/,
+ * which stays out of version control.  Used to pin the oracle's
+ * restatement and to generate the golden fixtures in tests/golden/.
+ *
+ * Wrapped functions:
+ *   hostLevinLaplacian  Matting.cu:39-219
+ *   gaussSeidel_host    Solve.cpp:3-33
+ *   jacobi_host         Solve.cpp:35-85
+ * The reference's GPU kernels are compiled along with Matting.cu but never
+ * launched: with its 25-band store they index shared memory out of bounds
+ * (BandedMatrix.cu:111,119).
+ */
+#include "Matting.cu"
+#include "Solve.h"
+
+extern "C" {
+
+void ref_hostLevinLaplacian(float* a, size_t apitch, int* bands, float* b, float lambda,
+                            const float* im4, const unsigned char* scribs,
+                            int W, int H, size_t imPitch)
+{
+    BandedMatrix L;
+    L.a = a;
+    L.apitch = apitch;
+    L.bands = bands;
+    L.nbands = 25;
+    L.rows = W * H;
+    L.cols = W * H;
+    hostLevinLaplacian(L, b, lambda, (float4*)im4, (unsigned char*)scribs, W, H, imPitch);
+}
+
+void ref_gaussSeidel_host(float* x, float* a, size_t apitch, int* bands, int nbands,
+                          int rows, const float* b, size_t iterations)
+{
+    BandedMatrix A;
+    A.a = a;
+    A.apitch = apitch;
+    A.bands = bands;
+    A.nbands = nbands;
+    A.rows = rows;
+    A.cols = rows;
+    gaussSeidel_host(x, A, b, iterations);
+}
+
+/* jacobi_host frees its caller's buffer after an odd number of iterations
+ * (Solve.cpp:72-83), so only even counts are accepted here.  Returns 0 on
+ * success, -1 when refused. */
+int ref_jacobi_host(float* x, float* a, size_t apitch, int* bands, int nbands,
+                    int rows, const float* b, size_t iterations, int xpad, float omega)
+{
+    if (iterations % 2 != 0) return -1;
+    BandedMatrix A;
+    A.a = a;
+    A.apitch = apitch;
+    A.bands = bands;
+    A.nbands = nbands;
+    A.rows = rows;
+    A.cols = rows;
+    jacobi_host(x, A, b, iterations, xpad, omega);
+    return 0;
+}
+
+}

@@ -1,0 +1,194 @@
+"""The CPU oracle, pinned against the reference's own outputs (golden
+fixtures made by tests/golden/make_golden.py from the compiled reference) and
+against independent numpy / scipy restatements."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from gpumatting_b200.synth import make_problem
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_ref32_restatement_bit_exact_vs_reference(orc, case):
+    g = load_golden(case)
+    a, b = orc.levin_ref32(g["im4"], g["scribbles"], float(g["lam"]), 1.0)
+    assert np.array_equal(a.view(np.uint32), g["a"].view(np.uint32))
+    assert np.array_equal(b.view(np.uint32), g["b"].view(np.uint32))
+
+
+def test_ref32_vs_compiled_reference_fresh_inputs(orc):
+    if not orc.ref_available():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    for (W, H, seed) in [(13, 11, 21), (40, 9, 22), (6, 30, 23)]:
+        p = make_problem(W, H, seed)
+        a1, b1 = orc.levin_ref32(p.image_float4(), p.scribbles, 1e-4, 1.0)
+        a2, b2 = orc.ref_levin(p.image_float4(), p.scribbles, 1e-4)
+        assert np.array_equal(a1.view(np.uint32), a2.view(np.uint32))
+        assert np.array_equal(b1, b2)
+
+
+def numpy_levin_fp64(img_u8: np.ndarray, eps: float) -> np.ndarray:
+    """Independent vectorised FP64 Levin Laplacian (getLevinLapRaster.m:22-62)
+    in the 25-band layout, L = D - A, no scribbles."""
+    H, W, _ = img_u8.shape
+    I = img_u8.astype(np.float64) / 255.0
+    N = W * H
+    bands = np.zeros((25, N))
+    cu = np.arange(1, W - 1)
+    cv = np.arange(1, H - 1)
+    win = np.stack([I[cv[:, None] + dv, cu[None, :] + du] for dv in (-1, 0, 1) for du in (-1, 0, 1)], axis=2)
+    mu = win.mean(axis=2, keepdims=True)
+    X = win - mu
+    cov = np.einsum("abki,abkj->abij", win, win) / 9 - np.einsum("abki,abkj->abij", mu, mu) + eps / 9 * np.eye(3)
+    T = (1 + np.einsum("abki,abij,ablj->abkl", X, np.linalg.inv(cov), X)) / 9
+    pos = [(du, dv) for dv in (-1, 0, 1) for du in (-1, 0, 1)]
+    vv, uu = np.meshgrid(cv, cu, indexing="ij")
+    for a_, (du1, dv1) in enumerate(pos):
+        ii = ((uu + du1) + (vv + dv1) * W).ravel()
+        for b_, (du2, dv2) in enumerate(pos):
+            k = 12 + (du2 - du1) + 5 * (dv2 - dv1)
+            np.add.at(bands[k], ii, -T[:, :, a_, b_].ravel())
+    bands[12] -= bands.sum(axis=0)
+    return bands
+
+
+@pytest.mark.parametrize("W,H,eps", [(23, 17, 1e-5), (9, 31, 1e-7), (5, 5, 1e-3)])
+def test_sym64_matches_independent_numpy(orc, W, H, eps):
+    p = make_problem(W, H, 11)
+    w = orc.levin_sym64(p.image.astype(np.float64) / 255.0, eps)
+    a = orc.sym_to_bands64(w, None, W, H)
+    ref = numpy_levin_fp64(p.image, eps)
+    scale = np.abs(ref).max()
+    assert np.abs(a - ref).max() <= 1e-10 * scale
+
+
+@pytest.mark.parametrize("case", ["s37x29", "data05"])
+def test_sym64_agrees_with_reference_where_float_is_accurate(orc, case):
+    """At lambda = 1e-2 the reference's FP32 arithmetic is accurate to a few
+    ulps, so its bands and the FP64 restatement must agree closely."""
+    g = load_golden(case)
+    im3 = g["im4"][..., :3].astype(np.float64)
+    H, W = g["scribbles"].shape
+    w = orc.levin_sym64(im3, float(g["lam"]))
+    gam = np.where((g["scribbles"] == 0) | (g["scribbles"] == 255), 1.0, 0.0).ravel()
+    a = orc.sym_to_bands64(w, gam, W, H)
+    ref = g["a"].astype(np.float64)
+    assert np.abs(a - ref).max() <= 2e-5 * np.abs(ref).max()
+    b = np.where(g["scribbles"].ravel() == 255, 1.0, 0.0)
+    assert np.array_equal(b, g["b"].astype(np.float64))
+
+
+def test_laplacian_structure(orc):
+    W, H = 19, 14
+    p = make_problem(W, H, 2)
+    w = orc.levin_sym64(p.image.astype(np.float64) / 255.0, 1e-5)
+    g = p.gamma.ravel().astype(np.float64)
+    a = orc.sym_to_bands64(w, g, W, H)
+    assert np.allclose(a.sum(axis=0), g, atol=1e-9 * np.abs(a).max())
+    offs = orc.levin_offsets(W)
+    for k in range(1, 13):  # L(i, i+o) == L(i+o, i)
+        o = offs[12 + k]
+        assert np.array_equal(a[12 + k][: W * H - o], a[12 - k][o:])
+    x = np.random.default_rng(0).normal(size=W * H)
+    op_s = orc.Operator(W=W, H=H, w=w, gamma=g)
+    op_b = orc.Operator(W=W, H=H, bands=a, offs=offs)
+    assert np.allclose(op_s.apply(x), op_b.apply(x), rtol=0, atol=1e-10 * np.abs(a).max())
+
+
+def test_cg64_matches_direct_solve(orc):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    W, H = 48, 32
+    p = make_problem(W, H, 3)
+    w = orc.levin_sym64(p.image.astype(np.float64) / 255.0, p.eps)
+    g = p.gamma.ravel().astype(np.float64)
+    b = (p.gamma * p.s).ravel().astype(np.float64)
+    a = orc.sym_to_bands64(w, g, W, H)
+    offs = orc.levin_offsets(W)
+    N = W * H
+    rows, cols, vals = [], [], []
+    for k in range(25):
+        i = np.arange(N)
+        j = i + offs[k]
+        m = (j >= 0) & (j < N) & (a[k] != 0)
+        rows.append(i[m]); cols.append(j[m]); vals.append(a[k][m])
+    M = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+    xs = spla.spsolve(M.tocsc(), b)
+    op = orc.Operator(W=W, H=H, w=w, gamma=g)
+    x, it, rel = op.cg(b, np.full(N, 0.5), rtol=1e-12, maxit=20000)
+    assert rel <= 1e-12
+    assert np.abs(x - xs).max() <= 1e-6
+    opb = orc.Operator(W=W, H=H, bands=a, offs=offs)
+    x2, it2, rel2 = opb.cg(b, np.full(N, 0.5), rtol=1e-12, maxit=20000)
+    assert np.abs(x2 - xs).max() <= 1e-6
+
+
+def test_gd64_and_jacobi64_reduce_residual(orc):
+    W, H = 20, 16
+    p = make_problem(W, H, 4)
+    w = orc.levin_sym64(p.image.astype(np.float64) / 255.0, p.eps)
+    g = p.gamma.ravel().astype(np.float64)
+    b = (p.gamma * p.s).ravel().astype(np.float64)
+    op = orc.Operator(W=W, H=H, w=w, gamma=g)
+    x0 = np.full(W * H, 0.5)
+    r0 = np.linalg.norm(b - op.apply(x0)) / np.linalg.norm(b)
+    _, _, rg = op.gd(b, x0, maxit=50)
+    _, _, rj = op.jacobi(b, x0, maxit=50)
+    assert rg < r0 and rj < r0
+    # one damped Jacobi step by hand
+    a = orc.sym_to_bands64(w, g, W, H)
+    x1, _, _ = op.jacobi(b, x0, omega=0.6, maxit=1)
+    assert np.allclose(x1, x0 + 0.6 * (b - op.apply(x0)) / a[12], rtol=1e-13, atol=1e-15)
+
+
+def test_solve_host_restatement_vs_reference():
+    g = load_golden("s37x29")
+    s = load_golden("s37x29", "solve_host_")
+    from oracle import oracle as O
+
+    H, W = g["scribbles"].shape
+    offs = O.levin_offsets(W)
+    gs = O.gs_host(g["a"], offs, g["b"], s["x0"], int(s["iters"]))
+    jac = O.jacobi_host(g["a"], offs, g["b"], s["x0"], int(s["iters"]), float(s["omega"]))
+    assert np.array_equal(gs, s["gs"])
+    assert np.array_equal(jac, s["jacobi"])
+
+
+def test_kat_banded_matrix(orc):
+    """tests/BandedMatrixTest.cu:41-114: N = 1e6, bands {-10, 0, 10} of ones
+    (zero where out of range), x_i = i."""
+    N = 1_000_000
+    a = np.ones((3, N))
+    a[0, :10] = 0
+    a[2, N - 10:] = 0
+    x = np.arange(N, dtype=np.float64)
+    y = orc.Operator(W=N, H=1, bands=a, offs=np.array([-10, 0, 10])).apply(x)
+    i = np.arange(N)
+    expect = np.where(i < 10, 10 + 2 * i, np.where(i < N - 10, 30 + 3 * (i - 10), 1999970 + 2 * (i - (N - 10))))
+    assert np.array_equal(y, expect.astype(np.float64))
+
+
+def test_compute_error_matches_formula(orc):
+    rng = np.random.default_rng(5)
+    al = rng.uniform(-0.3, 1.3, size=(17, 23)).astype(np.float32)
+    gt = rng.uniform(0, 1, size=(17, 23)).astype(np.float32)
+    d = np.where(al > 1, np.float32(1) - gt, np.where(al < 0, gt, al - gt)).astype(np.float32)
+    ref = np.mean((d * d).astype(np.float64))  # float products, double sum (main.cu:567-572)
+    assert abs(orc.compute_error(al, gt) - ref) <= 1e-12
+
+
+def test_assembly_adjoint_matches_finite_differences(orc):
+    """d/dI of sum_k gw_k . w_k(I) (orc_levin_backward64) vs central FD."""
+    W, H, eps = 9, 8, 1e-3
+    rng = np.random.default_rng(7)
+    im = rng.uniform(0.1, 0.9, size=(H, W, 3))
+    gw = rng.normal(size=(12, W * H))
+    dI = orc.levin_backward64(gw, im, eps)
+    h = 1e-6
+    for (v, u, c) in [(0, 0, 0), (3, 4, 1), (7, 8, 2), (4, 2, 0), (5, 6, 2)]:
+        ip, im_ = im.copy(), im.copy()
+        ip[v, u, c] += h
+        im_[v, u, c] -= h
+        fd = (np.sum(gw * orc.levin_sym64(ip, eps)) - np.sum(gw * orc.levin_sym64(im_, eps))) / (2 * h)
+        assert abs(fd - dI[v, u, c]) <= 1e-6 * max(1.0, abs(fd))

@@ -290,6 +290,8 @@ def run_ours(args):
     store = api.LevinStore(W, H, args.precision)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MB > L2
     params = dict(rtol=1e-6, max_iters=5000, replace_every=50)
+    if args.fixed_iters:
+        params = dict(rtol=0.0, max_iters=args.fixed_iters, replace_every=50)
 
     def step_device():
         store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
@@ -327,7 +329,7 @@ def run_ours(args):
     barrier(world)
     clk = clocks.stop()
     for r in res:
-        assert r.status == 0 and r.rel_residual <= 1e-6, r
+        assert r.status == 0 and (args.fixed_iters or r.rel_residual <= 1e-6), r
     iters = sum(r.iters for r in res)
     reps = sum(r.replacements for r in res)
     kern_ms = sum(r.kernel_ms for r in res)
@@ -337,11 +339,14 @@ def run_ours(args):
     value = work / 1e6 / t_max
 
     # e2e through the C ABI with host buffers
-    for _ in range(max(1, args.warmup // 2)):
-        step_e2e()
-    barrier(world)
-    ms_e, res_e = timed(step_e2e, args.steps)
-    barrier(world)
+    if args.no_e2e:
+        ms_e, res_e = ms, res
+    else:
+        for _ in range(max(1, args.warmup // 2)):
+            step_e2e()
+        barrier(world)
+        ms_e, res_e = timed(step_e2e, args.steps)
+        barrier(world)
     iters_e = sum(r.iters for r in res_e)
     te_max = allreduce_max(sum(ms_e) / 1000.0, world)
     e2e_value = allreduce_sum(N * iters_e, world) / 1e6 / te_max
@@ -437,6 +442,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--fixed-iters", type=int, default=0, help="profiling: run exactly this many CG iterations")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -96,9 +96,9 @@ static int check_bm(const BandedMatrix& a)
 // ---------------------------------------------------------------------------
 __global__ void gen_scalars_kernel(const double* part, int nb, double* sc, int slot)
 {
-    __shared__ double bc[1];
+    __shared__ double red[32];
     double t[1];
-    grid_total<1>(part, nb, t, bc);
+    grid_total<1>(part, nb, t, red);
     if (threadIdx.x == 0) sc[slot] = t[0];
 }
 
@@ -149,16 +149,16 @@ __global__ void gen_residual_kernel(float* __restrict__ r, float* __restrict__ p
     }
     block_sum<2>(acc, red);
     if (threadIdx.x == 0) {
-        part[blockIdx.x * 2] = acc[0];
-        part[blockIdx.x * 2 + 1] = acc[1];
+        part[blockIdx.x] = acc[0];
+        part[gridDim.x + blockIdx.x] = acc[1];
     }
 }
 
 __global__ void gen_scalars2_kernel(const double* part, int nb, double* sc)
 {
-    __shared__ double bc[2];
+    __shared__ double red[64];
     double t[2];
-    grid_total<2>(part, nb, t, bc);
+    grid_total<2>(part, nb, t, red);
     if (threadIdx.x == 0) { sc[0] = t[0]; sc[3] = t[1]; }
 }
 

@@ -238,26 +238,42 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch /* >=
     __syncthreads();
 }
 
-// Sums partials[0..n) (stride NV, component k) in a fixed order using warp
-// 0 of the calling block; every CTA that calls this with the same data gets
-// bit-identical results.  Reads bypass L1 (other CTAs wrote the data).
+// Sums the per-CTA partials p[k * n + i] (i < n) of each component k in a
+// fixed order: thread t adds entries t, t + T, t + 2T, ... (T = blockDim.x),
+// then a fixed shuffle tree and the warp sums in warp order.  Every CTA that
+// calls this on the same data gets bit-identical results.  All loads are
+// independent and coalesced; they bypass L1 (other CTAs wrote the data).
 template <int NV>
-__device__ __forceinline__ void grid_total(const double* partials, int n, double (&out)[NV], double* bcast)
+__device__ __forceinline__ void grid_total(const double* p, int n, double (&out)[NV], double* scratch /* >= 32*NV */)
 {
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x < 32) {
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = 0.0;
+    const int T = blockDim.x;
+    int i = threadIdx.x;
+    for (; i + T < n; i += 2 * T) {
+        double a[NV], b[NV];
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            double x = 0.0;
-            for (int i = lane; i < n; i += 32) x += __ldcg(partials + (size_t)i * NV + k);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) bcast[k] = x;
+            a[k] = __ldcg(p + (size_t)k * n + i);
+            b[k] = __ldcg(p + (size_t)k * n + i + T);
         }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] += a[k] + b[k];
+    }
+    if (i < n) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] += __ldcg(p + (size_t)k * n + i);
+    }
+    block_sum<NV>(v, scratch);
+    __shared__ double bc[NV];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) bc[k] = v[k];
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = bcast[k];
+    for (int k = 0; k < NV; ++k) out[k] = bc[k];
     __syncthreads();
 }
 

@@ -128,14 +128,15 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     unsigned char* bring = smem + L.bring_off;
     const int W = A.W, P = A.P;
 
-    // Tensor maps of this sweep's row loads.
-    const CUtensorMap* vm[3] = {nullptr, nullptr, nullptr};
+    // Tensor maps of this sweep's row loads (slot order fixed by plan_layout).
+    const CUtensorMap* vm[4] = {nullptr, nullptr, nullptr, nullptr};
     if (KIND == KIND_KRYLOV) {
-        vm[0] = &A.m_r[s.c]; vm[1] = &A.m_q[s.c]; vm[2] = &A.m_p[s.c];
+        vm[0] = &A.m_r[s.c]; vm[1] = &A.m_q[s.c]; vm[2] = &A.m_p[s.c]; vm[3] = &A.m_xacc[s.xsel];
     } else if (KIND == KIND_REPLACE) {
         vm[0] = MIXED ? &A.m_base[s.xsel] : nullptr; vm[1] = &A.m_xacc[s.xsel]; vm[2] = &A.m_p[s.c];
+        vm[3] = &A.m_b;
     } else {
-        vm[0] = &A.m_xacc[s.xsel];
+        vm[0] = &A.m_xacc[s.xsel]; vm[3] = &A.m_b;
     }
     const bool use_hi = KIND != KIND_KRYLOV;
     const CUtensorMap* bm = use_hi ? &A.m_whi : &A.m_wlo;
@@ -144,11 +145,11 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     auto issue_vec = [&](int j) {
         const int slot = j % K.Rv;
         uint64_t* bar = &bars[slot];
-        uint32_t bytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2];
+        uint32_t bytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2] + K.vbytes[3];
         mbar_arrive_expect_tx(bar, bytes);
         unsigned char* dst = vring + slot * K.vslot;
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+        for (int i = 0; i < 4; ++i)
             if (K.vbytes[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, v0 - 2 + j, bar);
     };
     auto issue_band = [&](int m) {
@@ -198,7 +199,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                     rring[(j & 3) * cw + tid - 2] = rn;
                     A.r[s.c ^ 1][gi] = rn;
                     A.p[s.c ^ 1][gi] = pn;
-                    if (!s.skipR) A.xacc[s.xsel][gi] = fmaf(s.af, pv, A.xacc[s.xsel][gi]);
+                    if (!s.skipR)
+                        A.xacc[s.xsel][gi] = fmaf(s.af, pv, reinterpret_cast<const float*>(vs_ptr + K.voff[3])[cc]);
                     part[0] += (double)rn * (double)rn;
                 }
             } else if (KIND == KIND_REPLACE) {
@@ -223,6 +225,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
             } else {  // Jacobi
                 pring_f[(j % 6) * bw + cc] = reinterpret_cast<const float*>(vs_ptr + K.voff[0])[cc];
             }
+            if (KIND != KIND_KRYLOV && tid >= 2 && tid < cw + 2)
+                rring[(j & 3) * cw + tid - 2] = reinterpret_cast<const float*>(vs_ptr + K.voff[3])[cc];
         }
         __syncthreads();
         if (*s_abort) return;  // uniform: read after the barrier by every thread
@@ -273,7 +277,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                     y = sym_apply<float, double, double>(prow, brow, K.pstride, K.gamma_off, cc);
                 else
                     y = ref25_apply<double, double>(prow, brow[0], K.pstride, cc);
-                const double bv = (double)A.b[(size_t)v * A.bpitch + u];
+                const double bv = (double)rring[((j - 2) & 3) * cw + tid];
                 const float rf = (float)(bv - y);
                 A.r[s.c][go] = rf;
                 part[0] += (double)rf * (double)rf;
@@ -291,7 +295,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                     y = ref25_apply<float, float>(prow, brow[0], K.pstride, cc);
                     dg = reinterpret_cast<const float*>(brow[0] + 12 * K.pstride)[cc];
                 }
-                const float bv = A.b[(size_t)v * A.bpitch + u];
+                const float bv = rring[((j - 2) & 3) * cw + tid];
                 const float rv = bv - y;
                 const float x0 = prow[2][cc];
                 A.xacc[s.xsel ^ 1][go] = x0 + A.omega * rv / dg;
@@ -306,7 +310,6 @@ template <class TLo, int OPLO, int OPHI, bool MIXED>
 __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant__ SolverArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ double bcast[kNPart];
     const int tid = threadIdx.x;
     const Layout& L = A.lay;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
@@ -347,6 +350,7 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
                 A.p[0][i] = 0.f;
                 A.q[0][i] = 0.f;
                 A.r[0][i] = 0.f;
+                A.bw[i] = A.b[(size_t)v * A.bpitch + u];
             }
     }
     const unsigned G = gridDim.x;
@@ -375,15 +379,15 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
                 run_sweep<TLo, OPLO, OPHI, MIXED, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, vphase, bphase);
         }
         block_sum<kNPart>(part, red);
-        double* slot = A.partials + ((size_t)parity * G + blockIdx.x) * kNPart;
+        double* slot = A.partials + (size_t)parity * G * kNPart + blockIdx.x;
         if (tid == 0) {
 #pragma unroll
-            for (int k = 0; k < kNPart; ++k) slot[k] = part[k];
+            for (int k = 0; k < kNPart; ++k) slot[(size_t)k * G] = part[k];
         }
         ok = grid_sync(A.gb, G, A.limit_ns);
         if (!ok) break;
         double tot[kNPart];
-        grid_total<kNPart>(A.partials + (size_t)parity * G * kNPart, (int)G, tot, bcast);
+        grid_total<kNPart>(A.partials + (size_t)parity * G * kNPart, (int)G, tot, red);
         parity ^= 1;
 
         if (kind == KIND_KRYLOV) {

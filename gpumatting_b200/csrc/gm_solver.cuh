@@ -22,8 +22,8 @@ struct KindLayout {
     int Rv, Rb;     // ring slots
     int vslot;      // bytes per vector slot
     int bslot;      // bytes per band slot
-    int voff[3];    // offsets of the vector arrays inside a vector slot
-    int vbytes[3];  // TMA bytes of each vector row (0 = unused)
+    int voff[4];    // offsets of the vector arrays inside a vector slot
+    int vbytes[4];  // TMA bytes of each vector row (0 = unused)
     int nvec;
     int planes;     // band planes loaded per row
     int pstride;    // bytes between planes inside a band slot (= bw * elem)
@@ -50,14 +50,15 @@ struct SolverOut {
 struct SolverArgs {
     // Tensor maps: vectors are 2-D {W, H}; bands 3-D {W, H, planes}.
     CUtensorMap m_r[2], m_q[2], m_p[2], m_xacc[2], m_base[2];
-    CUtensorMap m_wlo, m_whi, m_gamma;
+    CUtensorMap m_wlo, m_whi, m_gamma, m_b;
     float* r[2];
     float* q[2];
     float* p[2];
     float* xacc[2];
     double* base[2];
-    const float* b;
+    const float* b;           // caller's right-hand side
     int bpitch;               // elements
+    float* bw;                // work copy of b, pitch P (read through m_b)
     const float* alpha_in;
     float* alpha_out;
     int alpha_pitch;          // elements
@@ -65,7 +66,7 @@ struct SolverArgs {
     int W, H;
     int nstrips, nseg, nunits;
     Layout lay;
-    double* partials;         // [2][grid][kNPart]
+    double* partials;         // [2][kNPart][grid]
     GridBarrier* gb;
     SolverOut* out;
     // parameters

@@ -33,9 +33,9 @@ __global__ void dot_partial_kernel(const float* __restrict__ x, const float* __r
 
 __global__ void dot_finish_kernel(const double* part, int nparts, float* outf, double* outd)
 {
-    __shared__ double bc[1];
+    __shared__ double red[32];
     double t[1];
-    grid_total<1>(part, nparts, t, bc);
+    grid_total<1>(part, nparts, t, red);
     if (threadIdx.x == 0) {
         if (outf) *outf = (float)t[0];
         if (outd) *outd = t[0];

@@ -192,8 +192,9 @@ def test_breakdown_status(orc):
     st.planes("gamma")[10, 10] = float("nan")
     torch.cuda.synchronize()
     alpha = torch.full((H, W), 0.5, device="cuda")
-    res = st.solve(alpha, "cg", rtol=1e-6)
-    assert res.status == L.GM_ERR_BREAKDOWN
+    with pytest.raises(L.GmError) as e:
+        st.solve(alpha, "cg", rtol=1e-6)
+    assert e.value.status == L.GM_ERR_BREAKDOWN
 
 
 def test_bad_arguments():

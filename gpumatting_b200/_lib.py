@@ -46,7 +46,8 @@ class GmScribbles(C.Structure):
 
 class GmLevinStore(C.Structure):
     _fields_ = [("W", C.c_int), ("H", C.c_int), ("pitch", C.c_int), ("precision", C.c_int), ("w", C.c_void_p),
-                ("w32", C.c_void_p), ("gamma", C.c_void_p), ("b", C.c_void_p), ("owns", C.c_int)]
+                ("w32", C.c_void_p), ("gamma", C.c_void_p), ("b", C.c_void_p), ("d", C.c_void_p),
+                ("d32", C.c_void_p), ("owns", C.c_int)]
 
 
 class GmSolveParams(C.Structure):

@@ -265,6 +265,10 @@ class LevinStore:
             return _wrap(self.s.gamma, (H, P), torch.float32)
         if which == "b":
             return _wrap(self.s.b, (H, P), torch.float32)
+        if which == "d":
+            return _wrap(self.s.d, (H, P), torch.float32)
+        if which == "d32":
+            return _wrap(self.s.d32, (H, P), torch.float32)
         raise KeyError(which)
 
     def solve(self, alpha, solver: str = "cg", stream=None, **params) -> SolveResult:

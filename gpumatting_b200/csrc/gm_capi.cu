@@ -132,7 +132,7 @@ extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const g
     S.W = W;
     S.H = H;
     OpSource hi;
-    hi.kind = OP_SYM;
+    hi.kind = OP_SYMI;
     hi.dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     hi.esize = 4;
     hi.base = store->w32;
@@ -140,7 +140,9 @@ extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const g
     hi.plane_stride = (uint64_t)H * P * 4;
     hi.planes = 12;
     OpSource lo = hi;
-    if (p.use_low && store->precision != GM_PREC_FP32) {
+    lo.kind = OP_SYMD;
+    const bool low = p.use_low && store->precision != GM_PREC_FP32;
+    if (low) {
         lo.dt = store->precision == GM_PREC_FP16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
         lo.esize = 2;
         lo.base = store->w;
@@ -150,8 +152,10 @@ extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const g
     S.lo = lo;
     S.hi = hi;
     S.mixed = true;
-    S.gamma = store->gamma;
-    S.gamma_pitch = P;
+    S.xlo = low ? store->d : store->d32;
+    S.xlo_pitch = P;
+    S.xhi = store->gamma;
+    S.xhi_pitch = P;
     S.b = store->b;
     S.bpitch = P;
     S.alpha_in = alpha;

@@ -326,12 +326,42 @@ __global__ void __launch_bounds__(TW * TH) levin_ref_kernel(ImgView im, ScribVie
     if (bout) bout[i] = bv;
 }
 
+// d_i = gamma_i + sum of the affinities of row i as stored (upper planes at
+// i, lower ones at the neighbour), summed in FP64 and rounded once, for the
+// low-precision planes (d) and the FP32 planes (d32).
+template <class T>
+__global__ void levin_diag_kernel(const T* __restrict__ w, const float* __restrict__ w32,
+                                  const float* __restrict__ gamma, float* d, float* d32, int W, int H, int pitch)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W) return;
+    const size_t plane = (size_t)H * pitch;
+    const size_t i = (size_t)v * pitch + u;
+    double s = gamma[i], s32 = gamma[i];
+#pragma unroll
+    for (int k = 1; k <= 12; ++k) {
+        const int dv = (k + 2) / 5, du = k - 5 * dv;
+        s += (double)Cvt<T>::to_f(w[(k - 1) * plane + i]);
+        s32 += (double)w32[(k - 1) * plane + i];
+        const int ul = u - du, vl = v - dv;
+        if (ul >= 0 && ul < W && vl >= 0) {
+            const size_t j = (size_t)vl * pitch + ul;
+            s += (double)Cvt<T>::to_f(w[(k - 1) * plane + j]);
+            s32 += (double)w32[(k - 1) * plane + j];
+        }
+    }
+    d[i] = __double2float_rn(s);
+    d32[i] = __double2float_rn(s32);
+}
+
 template <class T>
 static void launch_sym(const ImgView& im, const ScribView& sc, double eps, int W, int H, const SymOut& o,
-                       cudaStream_t st)
+                       float* d, float* d32, cudaStream_t st)
 {
     dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH);
     levin_sym_kernel<T><<<grid, TW * TH, 0, st>>>(im, sc, eps, W, H, o);
+    dim3 g2((W + 127) / 128, H);
+    levin_diag_kernel<T><<<g2, 128, 0, st>>>(reinterpret_cast<const T*>(o.w), o.w32, o.gamma, d, d32, W, H, o.pitch);
 }
 
 }  // namespace gm
@@ -376,7 +406,7 @@ extern "C" int gm_levin_store_alloc(gm_levin_store* st, int W, int H, int precis
     const size_t b32 = (12 * plane * 4 + 255) & ~(size_t)255;
     const size_t b1 = (plane * 4 + 255) & ~(size_t)255;
     unsigned char* m = nullptr;
-    if (cudaMalloc((void**)&m, lo_bytes + b32 + 2 * b1) != cudaSuccess) {
+    if (cudaMalloc((void**)&m, lo_bytes + b32 + 4 * b1) != cudaSuccess) {
         gm_set_error_msg("store allocation failed");
         return GM_ERR_NOMEM;
     }
@@ -384,6 +414,8 @@ extern "C" int gm_levin_store_alloc(gm_levin_store* st, int W, int H, int precis
     st->w = precision == GM_PREC_FP32 ? (void*)m : (void*)(m + b32);
     st->gamma = (float*)(m + b32 + lo_bytes);
     st->b = (float*)(m + b32 + lo_bytes + b1);
+    st->d = (float*)(m + b32 + lo_bytes + 2 * b1);
+    st->d32 = (float*)(m + b32 + lo_bytes + 3 * b1);
     st->owns = 1;
     return GM_OK;
 }
@@ -399,7 +431,10 @@ extern "C" int gm_levin_store_free(gm_levin_store* st)
 extern "C" int gm_levin_assemble(gm_levin_store* st, const gm_image* im, const gm_scribbles* sc, double eps,
                                  BandedMatrix* bands25, float* b25, void* stream)
 {
-    if (!st || !st->w || !st->w32 || !st->gamma || !st->b) { gm_set_error_msg("store not allocated"); return GM_ERR_INVALID; }
+    if (!st || !st->w || !st->w32 || !st->gamma || !st->b || !st->d || !st->d32) {
+        gm_set_error_msg("store not allocated");
+        return GM_ERR_INVALID;
+    }
     if (!(eps >= 0.0)) { gm_set_error_msg("eps must be >= 0"); return GM_ERR_INVALID; }
     GM_TRY(gm_check_device(nullptr));
     ImgView iv;
@@ -423,9 +458,9 @@ extern "C" int gm_levin_assemble(gm_levin_store* st, const gm_image* im, const g
         o.b25 = b25;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    if (st->precision == GM_PREC_FP16) launch_sym<__half>(iv, sv, eps, st->W, st->H, o, s);
-    else if (st->precision == GM_PREC_BF16) launch_sym<__nv_bfloat16>(iv, sv, eps, st->W, st->H, o, s);
-    else launch_sym<float>(iv, sv, eps, st->W, st->H, o, s);
+    if (st->precision == GM_PREC_FP16) launch_sym<__half>(iv, sv, eps, st->W, st->H, o, st->d, st->d32, s);
+    else if (st->precision == GM_PREC_BF16) launch_sym<__nv_bfloat16>(iv, sv, eps, st->W, st->H, o, st->d, st->d32, s);
+    else launch_sym<float>(iv, sv, eps, st->W, st->H, o, st->d, st->d32, s);
     GM_CUDA_TRY(cudaGetLastError());
     return GM_OK;
 }

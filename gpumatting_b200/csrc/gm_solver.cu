@@ -4,27 +4,34 @@
 // Jacobi (the reference's cgSolve / gradSolve / jacobi, main.cu:406-556),
 // each run as ONE cooperative kernel with no host round trip per iteration.
 //
-// Work decomposition.  The image is cut into column strips of `cw` pixels
-// and each strip into row segments; one CTA owns one (strip, segment) unit
-// and sweeps down it row by row.  At every row step a single thread issues
-// TMA loads (cp.async.bulk.tensor, no multicast) of one halo'd row
-// (cw + 16 columns starting 8 left of the strip, zero fill outside the
-// image) of the input vectors and, two rows behind, of the band planes into
-// shared-memory rings completed on mbarriers.  Rows v-2..v+2 of the stencil
-// operand stay in a 6-row ring, so each band element and each vector
-// element is read from HBM once per sweep (plus the 2-row and 8-column
-// halos, which neighbouring CTAs read too and normally hit in L2).
+// Work decomposition.  The image is cut into column strips of kStrip (192)
+// pixels and each strip into row segments; one CTA owns one (strip,
+// segment) unit and sweeps down it row by row.  A CTA is one TMA producer
+// warp and kConsumers consumer warps:
+//   * the producer (one lane) streams, per row step, one halo'd row
+//     (kStrip + 16 columns from 8 left of the strip, zero fill outside the
+//     image) of the input vectors and of the band planes into shared-memory
+//     rings with cp.async.bulk.tensor (no multicast), each slot guarded by a
+//     "full" mbarrier (transaction bytes) and an "empty" mbarrier (one
+//     arrival per consumer warp) -- no block-wide barrier inside a sweep;
+//   * consumer warp w owns 64 output columns, two adjacent pixels per lane,
+//     and keeps rows v-2..v+2 of the stencil operand for its columns (+2 on
+//     each side) in a private 6-row ring, so only __syncwarp is needed.
+// Each band and vector element is read from HBM once per sweep (plus the
+// 2-row and 8-column halos, shared with neighbouring CTAs through L2).
 //
-// Operators.  OP_SYM: 12 planes of upper affinities w_k (k = du + 5 dv) plus
-// gamma; the lower half is read from the rows above (w_k(u-du, v-dv)) and
-// the Laplacian diagonal is implicit: y_i = gamma_i x_i + sum_j w_ij (x_i -
-// x_j), so rows sum to zero exactly whatever the storage precision.
-// OP_REF25: the reference's 25 explicit FP32 bands (main.cu:164-194).
+// Operators.  OP_SYMD (iteration operator of the symmetric store): 12 planes
+// of upper affinities w_k (k = du + 5 dv) and a diagonal plane d = gamma +
+// sum of the row's rounded affinities: y_i = d_i x_i - sum_j w_ij x_j, one
+// FMA per neighbour, rows still summing exactly to gamma.  OP_SYMI (true
+// operator, FP64 accumulation): y_i = gamma_i x_i + sum_j w_ij (x_i - x_j).
+// The lower half is read from the rows above (w_k(u-du, v-dv)).  OP_REF25:
+// the reference's 25 explicit FP32 bands (main.cu:164-194).
 //
 // CG iteration (one sweep, one grid barrier).  Sweep k, given alpha_{k-1}
 // and beta_k from the previous barrier, forms on the fly (halo included)
 //   r_k = r_{k-1} - alpha_{k-1} q_{k-1},  p_k = r_k + beta_k p_{k-1},
-// applies q_k = A p_k, adds alpha_{k-1} p_{k-1} into the local solution
+// applies q_k = A p_k, adds alpha_{k-1} p_{k-1} into the solution
 // increment, and reduces <r_k,r_k>, <p_k,q_k>, <r_k,q_k>, <q_k,q_k> in FP64.
 // After the barrier every CTA sums the per-CTA partials in the same fixed
 // order (bit-identical scalars everywhere): alpha_k = r.r / p.q and
@@ -35,12 +42,12 @@
 // Replacement sweep (every replace_every iterations, at restarts, when the
 // recursive residual drops below rtol, and at exit): folds the solution in
 // FP64 (x = base + increment + alpha p, halo included), recomputes the true
-// residual r = b - A_hi x with FP64 accumulation over the FP32 planes, and
+// residual r = b - A x with FP64 accumulation over the FP32 planes, and
 // writes alpha out.  With FP16/BF16 iteration planes this is the
 // reliable-update scheme that keeps the iterate converging to the FP32
 // operator's solution.
 //
-// Every wait (grid barrier, TMA row) has a wall-clock limit; on expiry the
+// Every wait (grid barrier, ring slot) has a wall-clock limit; on expiry the
 // kernel records GM_ERR_TIMEOUT and all CTAs leave their loops.
 #include "gm_solver.cuh"
 
@@ -49,57 +56,137 @@ namespace gm {
 __host__ __device__ constexpr int sym_dv(int k) { return (k + 2) / 5; }
 __host__ __device__ constexpr int sym_du(int k) { return k - 5 * ((k + 2) / 5); }
 
-// y = gamma x0 + sum_k w_k(u,v)(x0 - x(u+du,v+dv)) + w_k(u-du,v-dv)(x0 - x(u-du,v-dv))
-// prow[d]: operand row v+d-2; brow[d]: band slot of row v-d.
-template <class T, class V, class Acc>
-__device__ __forceinline__ Acc sym_apply(const V* const (&prow)[5], const unsigned char* const (&brow)[3],
-                                         int pstride, int gamma_off, int cc)
+// Two consecutive plane elements from an even index, as float2.
+__device__ __forceinline__ float2 ld2(const float* p, int i) { return *reinterpret_cast<const float2*>(p + i); }
+__device__ __forceinline__ float2 ld2(const __half* p, int i)
 {
-    const Acc x0 = static_cast<Acc>(prow[2][cc]);
-    const float* g = reinterpret_cast<const float*>(brow[0] + gamma_off);
-    Acc y = static_cast<Acc>(g[cc]) * x0;
-#pragma unroll
-    for (int k = 1; k <= 12; ++k) {
-        const int du = sym_du(k), dv = sym_dv(k);
-        const T* wu = reinterpret_cast<const T*>(brow[0] + (k - 1) * pstride);
-        const T* wl = reinterpret_cast<const T*>(brow[dv] + (k - 1) * pstride);
-        const Acc w1 = static_cast<Acc>(Cvt<T>::to_f(wu[cc]));
-        const Acc w2 = static_cast<Acc>(Cvt<T>::to_f(wl[cc - du]));
-        y += w1 * (x0 - static_cast<Acc>(prow[2 + dv][cc + du]));
-        y += w2 * (x0 - static_cast<Acc>(prow[2 - dv][cc - du]));
-    }
-    return y;
+    return __half22float2(*reinterpret_cast<const __half2*>(p + i));
+}
+__device__ __forceinline__ float2 ld2(const __nv_bfloat16* p, int i)
+{
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p + i));
+}
+// Two consecutive elements from an odd index: two aligned pair loads.
+__device__ __forceinline__ float2 ld2o(const float* p, int i) { return make_float2(p[i], p[i + 1]); }
+__device__ __forceinline__ float2 ld2o(const __half* p, int i)
+{
+    const __half2 a = *reinterpret_cast<const __half2*>(p + i - 1);
+    const __half2 b = *reinterpret_cast<const __half2*>(p + i + 1);
+    return __half22float2(__halves2half2(__high2half(a), __low2half(b)));
+}
+__device__ __forceinline__ float2 ld2o(const __nv_bfloat16* p, int i)
+{
+    const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(p + i - 1);
+    const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(p + i + 1);
+    return __bfloat1622float2(__halves2bfloat162(__high2bfloat16(a), __low2bfloat16(b)));
+}
+template <int DU, class T>
+__device__ __forceinline__ float2 ld2s(const T* p, int i)
+{
+    if constexpr ((DU & 1) == 0) return ld2(p, i);
+    else return ld2o(p, i);
 }
 
-// Diagonal of the symmetric operator: gamma + sum of the row's affinities.
 template <class T>
-__device__ __forceinline__ float sym_diag(const unsigned char* const (&brow)[3], int pstride, int gamma_off,
-                                          int cc)
+__device__ __forceinline__ const T* plane(const unsigned char* slot, int k, int pstride)
 {
-    float d = reinterpret_cast<const float*>(brow[0] + gamma_off)[cc];
-#pragma unroll
-    for (int k = 1; k <= 12; ++k) {
-        const int du = sym_du(k), dv = sym_dv(k);
-        d += Cvt<T>::to_f(reinterpret_cast<const T*>(brow[0] + (k - 1) * pstride)[cc]);
-        d += Cvt<T>::to_f(reinterpret_cast<const T*>(brow[dv] + (k - 1) * pstride)[cc - du]);
-    }
-    return d;
+    return reinterpret_cast<const T*>(slot + k * pstride);
 }
 
-// y = sum_{band j} a_j(u,v) x(u+du_j, v+dv_j), band j = 12 + du + 5 dv, in
-// band order (BandedMatrix.cu:172-173).
-template <class V, class Acc>
-__device__ __forceinline__ Acc ref25_apply(const V* const (&prow)[5], const unsigned char* b0, int pstride, int cc)
+// ---- operators on two adjacent output pixels (smem column c, c+1) ----
+// X[d][m]: operand at row v + d - 2, local column 2*lane + m (output pixel e
+// sits at m = 2 + e).  brow[d]: band slot of row v - d.
+template <class T, int K>
+__device__ __forceinline__ void symd_term(float& y0, float& y1, const float (&X)[5][6],
+                                          const unsigned char* const (&brow)[3], int pstride, int c)
 {
-    Acc y = 0;
+    constexpr int du = sym_du(K), dv = sym_dv(K);
+    const float2 wu = ld2(plane<T>(brow[0], K - 1, pstride), c);
+    y0 = fmaf(-wu.x, X[2 + dv][2 + du], y0);
+    y1 = fmaf(-wu.y, X[2 + dv][3 + du], y1);
+    const float2 wl = ld2s<du>(plane<T>(brow[dv], K - 1, pstride), c - du);
+    y0 = fmaf(-wl.x, X[2 - dv][2 - du], y0);
+    y1 = fmaf(-wl.y, X[2 - dv][3 - du], y1);
+}
+
+template <class T>
+__device__ __forceinline__ float2 symd_apply(const float (&X)[5][6], const unsigned char* const (&brow)[3], int pstride,
+                                             int xoff, int c)
+{
+    const float2 dg = ld2(reinterpret_cast<const float*>(brow[0] + xoff), c);
+    float y0 = dg.x * X[2][2], y1 = dg.y * X[2][3];
+    symd_term<T, 1>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 2>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 3>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 4>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 5>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 6>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 7>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 8>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 9>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 10>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 11>(y0, y1, X, brow, pstride, c);
+    symd_term<T, 12>(y0, y1, X, brow, pstride, c);
+    return make_float2(y0, y1);
+}
+
+// True operator, implicit diagonal, accumulation type V (float or double);
+// also returns the diagonal gamma + sum w (for Jacobi).
+template <class V, int K>
+__device__ __forceinline__ void symi_term(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
+                                          const unsigned char* const (&brow)[3], int pstride, int c)
+{
+    constexpr int du = sym_du(K), dv = sym_dv(K);
+    const float2 wu = ld2(plane<float>(brow[0], K - 1, pstride), c);
+    const float2 wl = ld2s<du>(plane<float>(brow[dv], K - 1, pstride), c - du);
+    y0 += (V)wu.x * (X[2][2] - X[2 + dv][2 + du]) + (V)wl.x * (X[2][2] - X[2 - dv][2 - du]);
+    y1 += (V)wu.y * (X[2][3] - X[2 + dv][3 + du]) + (V)wl.y * (X[2][3] - X[2 - dv][3 - du]);
+    d0 += (V)wu.x + (V)wl.x;
+    d1 += (V)wu.y + (V)wl.y;
+}
+
+template <class V>
+__device__ __forceinline__ void symi_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
+                                           const unsigned char* const (&brow)[3], int pstride, int xoff, int c)
+{
+    const float2 g = ld2(reinterpret_cast<const float*>(brow[0] + xoff), c);
+    y0 = (V)g.x * X[2][2];
+    y1 = (V)g.y * X[2][3];
+    d0 = (V)g.x;
+    d1 = (V)g.y;
+    symi_term<V, 1>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 2>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 3>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 4>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 5>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 6>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 7>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 8>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 9>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 10>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 11>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 12>(y0, y1, d0, d1, X, brow, pstride, c);
+}
+
+// Reference layout: y = sum_j a_j x(u+du_j, v+dv_j), band j = 12 + du + 5 dv,
+// in band order (BandedMatrix.cu:172-173); d = a_12.
+template <class V>
+__device__ __forceinline__ void ref25_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
+                                            const unsigned char* b0, int pstride, int c)
+{
+    y0 = 0;
+    y1 = 0;
 #pragma unroll
     for (int j = 0; j < 25; ++j) {
-        const int du = j % 5 - 2;   // j = 12 + du + 5 dv
-        const int dv = j / 5 - 2;
-        const float a = reinterpret_cast<const float*>(b0 + j * pstride)[cc];
-        y += static_cast<Acc>(a) * static_cast<Acc>(prow[2 + dv][cc + du]);
+        const int du = j % 5 - 2, dv = j / 5 - 2;
+        const float2 a = ld2(plane<float>(b0, j, pstride), c);
+        y0 += (V)a.x * X[2 + dv][2 + du];
+        y1 += (V)a.y * X[2 + dv][3 + du];
+        if (j == 12) {
+            d0 = (V)a.x;
+            d1 = (V)a.y;
+        }
     }
-    return y;
 }
 
 struct KState {
@@ -112,196 +199,332 @@ struct KState {
     int xsel;        // solution buffers read this sweep
 };
 
+// Per-thread pipeline state that lives across sweeps: one bit per ring slot.
+struct Pipe {
+    uint32_t full_v, full_b;    // consumers: parity of the next full-barrier phase
+    uint32_t empty_v, empty_b;  // producer: parity of the next empty-barrier phase
+    uint32_t used_v, used_b;    // producer: slot has been filled before
+};
+
+__device__ __forceinline__ int ring_next(int s, int R) { return s + 1 == R ? 0 : s + 1; }
+__device__ __forceinline__ int ring_prev(int s, int R) { return s == 0 ? R - 1 : s - 1; }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <class V>
+__device__ __forceinline__ void load_rows(V (&X)[5][6], const V* ring, int r0, int lc0)
+{
+    // rows v-2..v+2 sit in ring rows r0, r0+1, ... (mod 6); columns lc0..lc0+5
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+        int r = r0 + d;
+        r = r >= 6 ? r - 6 : r;
+        const V* row = ring + r * kRingCols + lc0;
+#pragma unroll
+        for (int m = 0; m < 6; m += 2) {
+            if constexpr (sizeof(V) == 4) {
+                const float2 t = *reinterpret_cast<const float2*>(row + m);
+                X[d][m] = t.x;
+                X[d][m + 1] = t.y;
+            } else {
+                const double2 t = *reinterpret_cast<const double2*>(row + m);
+                X[d][m] = t.x;
+                X[d][m + 1] = t.y;
+            }
+        }
+    }
+}
+
 template <class TLo, int OPLO, int OPHI, bool MIXED, int KIND>
 __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* smem, int u0, int v0, int v1,
-                                          const KState& s, double (&part)[kNPart], uint32_t& vphase,
-                                          uint32_t& bphase)
+                                          const KState& s, double (&part)[kNPart], Pipe& pp)
 {
     const Layout& L = A.lay;
     const KindLayout& K = L.k[KIND];
-    const int tid = threadIdx.x;
-    const int cw = L.cw, bw = L.bw;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nsteps = v1 - v0 + 4;
     const int nband = nsteps - 2;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     unsigned char* vring = smem + L.vring_off;
     unsigned char* bring = smem + L.bring_off;
-    const int W = A.W, P = A.P;
-
-    // Tensor maps of this sweep's row loads (slot order fixed by plan_layout).
-    const CUtensorMap* vm[4] = {nullptr, nullptr, nullptr, nullptr};
-    if (KIND == KIND_KRYLOV) {
-        vm[0] = &A.m_r[s.c]; vm[1] = &A.m_q[s.c]; vm[2] = &A.m_p[s.c]; vm[3] = &A.m_xacc[s.xsel];
-    } else if (KIND == KIND_REPLACE) {
-        vm[0] = MIXED ? &A.m_base[s.xsel] : nullptr; vm[1] = &A.m_xacc[s.xsel]; vm[2] = &A.m_p[s.c];
-        vm[3] = &A.m_b;
-    } else {
-        vm[0] = &A.m_xacc[s.xsel]; vm[3] = &A.m_b;
-    }
-    const bool use_hi = KIND != KIND_KRYLOV;
-    const CUtensorMap* bm = use_hi ? &A.m_whi : &A.m_wlo;
-    const bool sym = (use_hi ? OPHI : OPLO) == OP_SYM;
-
-    auto issue_vec = [&](int j) {
-        const int slot = j % K.Rv;
-        uint64_t* bar = &bars[slot];
-        uint32_t bytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2] + K.vbytes[3];
-        mbar_arrive_expect_tx(bar, bytes);
-        unsigned char* dst = vring + slot * K.vslot;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (K.vbytes[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, v0 - 2 + j, bar);
-    };
-    auto issue_band = [&](int m) {
-        const int slot = m % K.Rb;
-        uint64_t* bar = &bars[kRvMax + slot];
-        uint32_t bytes = K.bbytes + (sym ? bw * 4 : 0);
-        mbar_arrive_expect_tx(bar, bytes);
-        unsigned char* dst = bring + slot * K.bslot;
-        tma_load_3d(dst, bm, u0 - 8, v0 - 2 + m, 0, bar);
-        if (sym) tma_load_2d(dst + K.gamma_off, &A.m_gamma, u0 - 8, v0 - 2 + m, bar);
-    };
-
-    if (tid == 0) {
-        fence_proxy_async();
-        const int nv = K.D < nsteps ? K.D : nsteps;
-        for (int j = 0; j < nv; ++j) issue_vec(j);
-        for (int m = 0; m < K.D - 2 && m < nband; ++m) issue_band(m);
-    }
-
-    float* pring_f = reinterpret_cast<float*>(smem + L.pring_off);
-    double* pring_d = reinterpret_cast<double*>(smem + L.pring_off);
-    float* rring = reinterpret_cast<float*>(smem + L.rring_off);
-
     volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + 32 * kNPart * 8);
+    constexpr bool kSymBand = (KIND == KIND_KRYLOV ? OPLO : OPHI) != OP_REF25;
+
+    if (warp == kConsumers) {
+        // ------------------------------ producer ------------------------------
+        if (lane != 0) return;
+        const CUtensorMap* vm[4] = {nullptr, nullptr, nullptr, nullptr};
+        if (KIND == KIND_KRYLOV) {
+            vm[0] = &A.m_r[s.c]; vm[1] = &A.m_q[s.c]; vm[2] = &A.m_p[s.c]; vm[3] = &A.m_xacc[s.xsel];
+        } else if (KIND == KIND_REPLACE) {
+            vm[0] = MIXED ? &A.m_base[s.xsel] : nullptr; vm[1] = &A.m_xacc[s.xsel]; vm[2] = &A.m_p[s.c];
+            vm[3] = &A.m_b;
+        } else {
+            vm[0] = &A.m_xacc[s.xsel]; vm[3] = &A.m_b;
+        }
+        const CUtensorMap* bm = KIND == KIND_KRYLOV ? &A.m_wlo : &A.m_whi;
+        const CUtensorMap* xm = KIND == KIND_KRYLOV ? &A.m_xlo : &A.m_xhi;
+        const uint32_t vbytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2] + K.vbytes[3];
+        fence_proxy_async();
+        int vs = 0, bs = 0;
+        for (int t = 0; t < nsteps; ++t) {
+            if (*s_abort) break;
+            const int row = v0 - 2 + t;
+            {
+                const uint32_t bit = 1u << vs;
+                if (pp.used_v & bit) {
+                    if (!mbar_wait_bounded(&empty[vs], (pp.empty_v & bit) ? 1u : 0u, A.gb, A.tma_limit_ns)) {
+                        *s_abort = 1;
+                        break;
+                    }
+                    pp.empty_v ^= bit;
+                }
+                pp.used_v |= bit;
+                unsigned char* dst = vring + vs * K.vslot;
+                mbar_arrive_expect_tx(&full[vs], vbytes);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (K.vbytes[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, row, &full[vs]);
+                vs = ring_next(vs, K.Rv);
+            }
+            if (t < nband) {
+                const uint32_t bit = 1u << bs;
+                if (pp.used_b & bit) {
+                    if (!mbar_wait_bounded(&empty[kRvMax + bs], (pp.empty_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns)) {
+                        *s_abort = 1;
+                        break;
+                    }
+                    pp.empty_b ^= bit;
+                }
+                pp.used_b |= bit;
+                unsigned char* dst = bring + bs * K.bslot;
+                mbar_arrive_expect_tx(&full[kRvMax + bs], K.bbytes);
+                tma_load_3d(dst, bm, u0 - 8, row, 0, &full[kRvMax + bs]);
+                if (K.xoff >= 0) tma_load_2d(dst + K.xoff, xm, u0 - 8, row, &full[kRvMax + bs]);
+                bs = ring_next(bs, K.Rb);
+            }
+        }
+        return;
+    }
+
+    // -------------------------------- consumers --------------------------------
+    const int w = warp;
+    const int c = 8 + kWarpCols * w + 2 * lane;        // smem column of this lane's pixel pair
+    const int lc0 = 2 * lane;                          // first operand column (local ring index)
+    const int u = u0 + kWarpCols * w + 2 * lane;       // image column of pixel 0
+    const bool in0 = u < A.W, in1 = u + 1 < A.W;
+    // extra operand pair for the ring halo: lane 0 left, lane 1 right
+    const bool has_x = lane < 2;
+    const int cx = lane == 0 ? 6 + kWarpCols * w : 8 + kWarpCols * w + kWarpCols;
+    const int lcx = lane == 0 ? 0 : kRingCols - 2;
+    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * 6 * kRingCols * 2;
+    double* ring_d = reinterpret_cast<double*>(smem + L.pring_off) + w * 6 * kRingCols;
+    float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * 4 * kWarpCols;  // r or b, own columns
+    const int P = A.P;
+
+    int vs = 0;       // vector slot of step j
+    int bs0 = 0;      // band slot of step j-2 (valid from j = 2)
+    int rj = 0;       // ring row of step j (j mod 6)
+    int oj = 0;       // own ring row of step j (j mod 4)
+    const int Rb = K.Rb;
     for (int j = 0; j < nsteps; ++j) {
         const int Lr = v0 - 2 + j;
         {
-            const int vs = j % K.Rv;
-            if (*s_abort || !mbar_wait_bounded(&bars[vs], (vphase >> vs) & 1u, A.gb, A.tma_limit_ns)) *s_abort = 1;
-            vphase ^= 1u << vs;
+            const uint32_t bit = 1u << vs;
+            if (!*s_abort && !mbar_wait_bounded(&full[vs], (pp.full_v & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
+                *s_abort = 1;
+            pp.full_v ^= bit;
         }
-        const unsigned char* vs_ptr = vring + (j % K.Rv) * K.vslot;
+        const unsigned char* vsp = vring + vs * K.vslot;
+        const bool own_row = Lr >= v0 && Lr < v1;
+        const size_t gi = (size_t)(own_row ? Lr : 0) * P + u;
         // ---------------- phase A: combine the incoming row ----------------
-        if (tid < cw + 4) {
-            const int cc = tid + 6;
-            const int uo = u0 + tid - 2;
-            const bool own = tid >= 2 && tid < cw + 2 && uo < W && Lr >= v0 && Lr < v1;
-            const size_t gi = (size_t)Lr * P + uo;
-            if (KIND == KIND_KRYLOV) {
-                const float rv = reinterpret_cast<const float*>(vs_ptr + K.voff[0])[cc];
-                const float qv = reinterpret_cast<const float*>(vs_ptr + K.voff[1])[cc];
-                const float pv = reinterpret_cast<const float*>(vs_ptr + K.voff[2])[cc];
-                const float rn = s.skipR ? rv : fmaf(-s.af, qv, rv);
-                const float pn = s.beta_zero ? rn : fmaf(s.bf, pv, rn);
-                pring_f[(j % 6) * bw + cc] = pn;
-                if (own) {
-                    rring[(j & 3) * cw + tid - 2] = rn;
-                    A.r[s.c ^ 1][gi] = rn;
-                    A.p[s.c ^ 1][gi] = pn;
-                    if (!s.skipR)
-                        A.xacc[s.xsel][gi] = fmaf(s.af, pv, reinterpret_cast<const float*>(vs_ptr + K.voff[3])[cc]);
-                    part[0] += (double)rn * (double)rn;
-                }
-            } else if (KIND == KIND_REPLACE) {
-                const float xv = reinterpret_cast<const float*>(vs_ptr + K.voff[1])[cc];
-                const float pv = reinterpret_cast<const float*>(vs_ptr + K.voff[2])[cc];
-                double xf;
-                if (MIXED) {
-                    const double bv = reinterpret_cast<const double*>(vs_ptr + K.voff[0])[cc];
-                    xf = bv + (double)xv + s.ad * (double)pv;
+        if (KIND == KIND_KRYLOV) {
+            const float* vr = reinterpret_cast<const float*>(vsp + K.voff[0]);
+            const float* vq = reinterpret_cast<const float*>(vsp + K.voff[1]);
+            const float* vp = reinterpret_cast<const float*>(vsp + K.voff[2]);
+            const float* vx = reinterpret_cast<const float*>(vsp + K.voff[3]);
+            auto combine = [&](int cc, float2& rn, float2& pv) {
+                const float2 rv = ld2(vr, cc);
+                pv = ld2(vp, cc);
+                if (s.skipR) {
+                    rn = rv;
                 } else {
-                    xf = (double)fmaf(s.af, pv, xv);
+                    const float2 qv = ld2(vq, cc);
+                    rn = make_float2(fmaf(-s.af, qv.x, rv.x), fmaf(-s.af, qv.y, rv.y));
                 }
-                pring_d[(j % 6) * bw + cc] = xf;
-                if (own) {
+                return s.beta_zero ? rn : make_float2(fmaf(s.bf, pv.x, rn.x), fmaf(s.bf, pv.y, rn.y));
+            };
+            float2 rn, pv;
+            const float2 pn = combine(c, rn, pv);
+            *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lc0 + 2) = pn;
+            if (has_x) {
+                float2 rx, px;
+                *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lcx) = combine(cx, rx, px);
+            }
+            if (own_row) {
+                *reinterpret_cast<float2*>(own_ring + oj * kWarpCols + lc0) = rn;
+                if (in1) {
+                    *reinterpret_cast<float2*>(A.r[s.c ^ 1] + gi) = rn;
+                    *reinterpret_cast<float2*>(A.p[s.c ^ 1] + gi) = pn;
+                    if (!s.skipR) {
+                        const float2 xv = ld2(vx, c);
+                        *reinterpret_cast<float2*>(A.xacc[s.xsel] + gi) =
+                            make_float2(fmaf(s.af, pv.x, xv.x), fmaf(s.af, pv.y, xv.y));
+                    }
+                    part[0] += (double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y;
+                } else if (in0) {
+                    A.r[s.c ^ 1][gi] = rn.x;
+                    A.p[s.c ^ 1][gi] = pn.x;
+                    if (!s.skipR) A.xacc[s.xsel][gi] = fmaf(s.af, pv.x, vx[c]);
+                    part[0] += (double)rn.x * (double)rn.x;
+                }
+            }
+        } else if (KIND == KIND_REPLACE) {
+            const float* vx = reinterpret_cast<const float*>(vsp + K.voff[1]);
+            const float* vp = reinterpret_cast<const float*>(vsp + K.voff[2]);
+            const float* vb = reinterpret_cast<const float*>(vsp + K.voff[3]);
+            auto fold = [&](int cc) {
+                const float2 xv = ld2(vx, cc), pv = ld2(vp, cc);
+                double2 xf;
+                if (MIXED) {
+                    const double2 bv = *reinterpret_cast<const double2*>(
+                        reinterpret_cast<const double*>(vsp + K.voff[0]) + cc);
+                    xf.x = bv.x + (double)xv.x + s.ad * (double)pv.x;
+                    xf.y = bv.y + (double)xv.y + s.ad * (double)pv.y;
+                } else {
+                    xf.x = (double)fmaf(s.af, pv.x, xv.x);
+                    xf.y = (double)fmaf(s.af, pv.y, xv.y);
+                }
+                return xf;
+            };
+            const double2 xf = fold(c);
+            *reinterpret_cast<double2*>(ring_d + rj * kRingCols + lc0 + 2) = xf;
+            if (has_x) *reinterpret_cast<double2*>(ring_d + rj * kRingCols + lcx) = fold(cx);
+            if (own_row) {
+                *reinterpret_cast<float2*>(own_ring + oj * kWarpCols + lc0) = ld2(vb, c);
+                if (in1) {
                     if (MIXED) {
-                        A.base[s.xsel ^ 1][gi] = xf;
+                        *reinterpret_cast<double2*>(A.base[s.xsel ^ 1] + gi) = xf;
+                        *reinterpret_cast<float2*>(A.xacc[s.xsel ^ 1] + gi) = make_float2(0.f, 0.f);
+                    } else {
+                        *reinterpret_cast<float2*>(A.xacc[s.xsel ^ 1] + gi) = make_float2((float)xf.x, (float)xf.y);
+                    }
+                } else if (in0) {
+                    if (MIXED) {
+                        A.base[s.xsel ^ 1][gi] = xf.x;
                         A.xacc[s.xsel ^ 1][gi] = 0.f;
                     } else {
-                        A.xacc[s.xsel ^ 1][gi] = (float)xf;
+                        A.xacc[s.xsel ^ 1][gi] = (float)xf.x;
                     }
                 }
-            } else {  // Jacobi
-                pring_f[(j % 6) * bw + cc] = reinterpret_cast<const float*>(vs_ptr + K.voff[0])[cc];
             }
-            if (KIND != KIND_KRYLOV && tid >= 2 && tid < cw + 2)
-                rring[(j & 3) * cw + tid - 2] = reinterpret_cast<const float*>(vs_ptr + K.voff[3])[cc];
+        } else {  // Jacobi
+            const float* vx = reinterpret_cast<const float*>(vsp + K.voff[0]);
+            const float* vb = reinterpret_cast<const float*>(vsp + K.voff[3]);
+            *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lc0 + 2) = ld2(vx, c);
+            if (has_x) *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lcx) = ld2(vx, cx);
+            if (own_row) *reinterpret_cast<float2*>(own_ring + oj * kWarpCols + lc0) = ld2(vb, c);
         }
-        __syncthreads();
-        if (*s_abort) return;  // uniform: read after the barrier by every thread
-        if (tid == 0) {
-            fence_proxy_async();
-            if (j + K.D < nsteps) issue_vec(j + K.D);
-            const int m = j + K.D - 2;
-            if (m >= 0 && m < nband) issue_band(m);
-        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[vs]);
+        vs = ring_next(vs, K.Rv);
         if (j >= 2) {
-            const int m = j - 2;
-            const int bs = m % K.Rb;
-            if (*s_abort || !mbar_wait_bounded(&bars[kRvMax + bs], (bphase >> bs) & 1u, A.gb, A.tma_limit_ns))
+            if (j > 2) bs0 = ring_next(bs0, Rb);
+            const uint32_t bit = 1u << bs0;
+            if (!*s_abort && !mbar_wait_bounded(&full[kRvMax + bs0], (pp.full_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
                 *s_abort = 1;
-            bphase ^= 1u << bs;
+            pp.full_b ^= bit;
         }
-        if (j < 4) continue;
-        // ---------------- phase B: stencil on output row v ----------------
-        const int v = Lr - 2;
-        const int u = u0 + tid;
-        if (tid < cw && u < W) {
-            const int cc = tid + 8;
-            const unsigned char* brow[3] = {bring + ((j - 2) % K.Rb) * K.bslot,
-                                            bring + ((j - 3) % K.Rb) * K.bslot,
-                                            bring + ((j - 4) % K.Rb) * K.bslot};
+        if (j >= 4) {
+            // ---------------- phase B: stencil on output row v ----------------
+            const int v = Lr - 2;
+            const int b1 = ring_prev(bs0, Rb), b2 = ring_prev(b1, Rb);
+            const unsigned char* brow[3] = {bring + bs0 * K.bslot, bring + b1 * K.bslot, bring + b2 * K.bslot};
+            int r0 = rj + 2;  // ring row of step j-4 = (j + 2) mod 6
+            r0 = r0 >= 6 ? r0 - 6 : r0;
+            int o2 = oj + 2;  // own ring row of step j-2
+            o2 = o2 >= 4 ? o2 - 4 : o2;
             const size_t go = (size_t)v * P + u;
-            if (KIND == KIND_KRYLOV) {
-                const float* prow[5];
-#pragma unroll
-                for (int d = 0; d < 5; ++d) prow[d] = pring_f + ((j - 4 + d) % 6) * bw;
-                float qv;
-                if (OPLO == OP_SYM)
-                    qv = sym_apply<TLo, float, float>(prow, brow, K.pstride, K.gamma_off, cc);
-                else
-                    qv = ref25_apply<float, float>(prow, brow[0], K.pstride, cc);
-                A.q[s.c ^ 1][go] = qv;
-                const float pn = prow[2][cc];
-                const float rn = rring[((j - 2) & 3) * cw + tid];
-                part[1] += (double)pn * (double)qv;
-                part[2] += (double)rn * (double)qv;
-                part[3] += (double)qv * (double)qv;
-            } else if (KIND == KIND_REPLACE) {
-                const double* prow[5];
-#pragma unroll
-                for (int d = 0; d < 5; ++d) prow[d] = pring_d + ((j - 4 + d) % 6) * bw;
-                double y;
-                if (OPHI == OP_SYM)
-                    y = sym_apply<float, double, double>(prow, brow, K.pstride, K.gamma_off, cc);
-                else
-                    y = ref25_apply<double, double>(prow, brow[0], K.pstride, cc);
-                const double bv = (double)rring[((j - 2) & 3) * cw + tid];
-                const float rf = (float)(bv - y);
-                A.r[s.c][go] = rf;
-                part[0] += (double)rf * (double)rf;
-                part[1] += bv * bv;
-                A.alpha_out[(size_t)v * A.alpha_pitch + u] = (float)prow[2][cc];
-            } else {  // Jacobi
-                const float* prow[5];
-#pragma unroll
-                for (int d = 0; d < 5; ++d) prow[d] = pring_f + ((j - 4 + d) % 6) * bw;
-                float y, dg;
-                if (OPHI == OP_SYM) {
-                    y = sym_apply<float, float, float>(prow, brow, K.pstride, K.gamma_off, cc);
-                    dg = sym_diag<float>(brow, K.pstride, K.gamma_off, cc);
-                } else {
-                    y = ref25_apply<float, float>(prow, brow[0], K.pstride, cc);
-                    dg = reinterpret_cast<const float*>(brow[0] + 12 * K.pstride)[cc];
+            if (in0) {
+                if (KIND == KIND_KRYLOV) {
+                    float X[5][6];
+                    load_rows<float>(X, ring_f, r0, lc0);
+                    float2 q;
+                    if (OPLO == OP_SYMD) {
+                        q = symd_apply<TLo>(X, brow, K.pstride, K.xoff, c);
+                    } else {
+                        float d0, d1;
+                        ref25_apply<float>(q.x, q.y, d0, d1, X, brow[0], K.pstride, c);
+                    }
+                    const float2 rn = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
+                    if (in1) {
+                        *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go) = q;
+                        part[1] += (double)X[2][2] * (double)q.x + (double)X[2][3] * (double)q.y;
+                        part[2] += (double)rn.x * (double)q.x + (double)rn.y * (double)q.y;
+                        part[3] += (double)q.x * (double)q.x + (double)q.y * (double)q.y;
+                    } else {
+                        A.q[s.c ^ 1][go] = q.x;
+                        part[1] += (double)X[2][2] * (double)q.x;
+                        part[2] += (double)rn.x * (double)q.x;
+                        part[3] += (double)q.x * (double)q.x;
+                    }
+                } else if (KIND == KIND_REPLACE) {
+                    double X[5][6];
+                    load_rows<double>(X, ring_d, r0, lc0);
+                    double y0, y1, d0, d1;
+                    if (OPHI == OP_REF25) ref25_apply<double>(y0, y1, d0, d1, X, brow[0], K.pstride, c);
+                    else symi_apply<double>(y0, y1, d0, d1, X, brow, K.pstride, K.xoff, c);
+                    const float2 bv = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
+                    const float r0f = (float)((double)bv.x - y0), r1f = (float)((double)bv.y - y1);
+                    float* ao = A.alpha_out + (size_t)v * A.alpha_pitch + u;
+                    ao[0] = (float)X[2][2];
+                    A.r[s.c][go] = r0f;
+                    part[0] += (double)r0f * (double)r0f;
+                    part[1] += (double)bv.x * (double)bv.x;
+                    if (in1) {
+                        ao[1] = (float)X[2][3];
+                        A.r[s.c][go + 1] = r1f;
+                        part[0] += (double)r1f * (double)r1f;
+                        part[1] += (double)bv.y * (double)bv.y;
+                    }
+                } else {  // Jacobi
+                    float X[5][6];
+                    load_rows<float>(X, ring_f, r0, lc0);
+                    float y0, y1, d0, d1;
+                    if (OPHI == OP_REF25) ref25_apply<float>(y0, y1, d0, d1, X, brow[0], K.pstride, c);
+                    else symi_apply<float>(y0, y1, d0, d1, X, brow, K.pstride, K.xoff, c);
+                    const float2 bv = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
+                    const float rv0 = bv.x - y0, rv1 = bv.y - y1;
+                    A.xacc[s.xsel ^ 1][go] = X[2][2] + A.omega * rv0 / d0;
+                    part[0] += (double)rv0 * (double)rv0;
+                    part[1] += (double)bv.x * (double)bv.x;
+                    if (in1) {
+                        A.xacc[s.xsel ^ 1][go + 1] = X[2][3] + A.omega * rv1 / d1;
+                        part[0] += (double)rv1 * (double)rv1;
+                        part[1] += (double)bv.y * (double)bv.y;
+                    }
                 }
-                const float bv = rring[((j - 2) & 3) * cw + tid];
-                const float rv = bv - y;
-                const float x0 = prow[2][cc];
-                A.xacc[s.xsel ^ 1][go] = x0 + A.omega * rv / dg;
-                part[0] += (double)rv * (double)rv;
-                part[1] += (double)bv * (double)bv;
             }
+            __syncwarp();
+            // release the band row whose last use this was
+            if (lane == 0) mbar_arrive(&empty[kRvMax + (kSymBand ? b2 : bs0)]);
+        } else if (j >= 2 && !kSymBand) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[kRvMax + bs0]);  // rows v0-2, v0-1: unused by ref25
+        }
+        rj = rj + 1 == 6 ? 0 : rj + 1;
+        oj = (oj + 1) & 3;
+    }
+    // band rows of the last two steps are never the v-2 row of a later step
+    if (kSymBand && nsteps >= 4) {
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[kRvMax + bs0]);
+            mbar_arrive(&empty[kRvMax + ring_prev(bs0, Rb)]);
         }
     }
 }
@@ -312,32 +535,37 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;
     const Layout& L = A.lay;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     double* red = reinterpret_cast<double*>(smem + L.red_off);
 
     const int unit = blockIdx.x;
     int u0 = 0, v0 = 0, v1 = 0;
     if (unit < A.nunits) {
         const int st = unit % A.nstrips, sg = unit / A.nstrips;
-        u0 = st * L.cw;
+        u0 = st * kStrip;
         v0 = (int)((long long)A.H * sg / A.nseg);
         v1 = (int)((long long)A.H * (sg + 1) / A.nseg);
     }
     const bool active = v1 > v0;
 
     if (tid == 0) {
-        for (int i = 0; i < kRvMax + kRbMax; ++i) mbar_init(&bars[i], 1);
+        for (int i = 0; i < kRvMax + kRbMax; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kConsumers);
+        }
         *reinterpret_cast<volatile int*>(smem + L.red_off + 32 * kNPart * 8) = 0;
         fence_mbar_init();
     }
     __syncthreads();
-    uint32_t vphase = 0, bphase = 0;
+    Pipe pp = {0u, 0u, 0u, 0u, 0u, 0u};
 
     const bool jac = A.solver == GM_SOLVER_JACOBI;
-    // Import the initial guess; zero the first search direction.
+    // Import the initial guess and the right-hand side; zero the first
+    // search direction.
     if (active) {
         for (int v = v0; v < v1; ++v)
-            for (int cl = tid; cl < L.cw; cl += blockDim.x) {
+            for (int cl = tid; cl < kStrip; cl += blockDim.x) {
                 const int u = u0 + cl;
                 if (u >= A.W) continue;
                 const size_t i = (size_t)v * A.P + u;
@@ -372,11 +600,11 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
         double part[kNPart] = {0.0, 0.0, 0.0, 0.0};
         if (active) {
             if (kind == KIND_KRYLOV)
-                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_KRYLOV>(A, smem, u0, v0, v1, s, part, vphase, bphase);
+                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_KRYLOV>(A, smem, u0, v0, v1, s, part, pp);
             else if (kind == KIND_REPLACE)
-                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_REPLACE>(A, smem, u0, v0, v1, s, part, vphase, bphase);
+                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_REPLACE>(A, smem, u0, v0, v1, s, part, pp);
             else
-                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, vphase, bphase);
+                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, pp);
         }
         block_sum<kNPart>(part, red);
         double* slot = A.partials + (size_t)parity * G * kNPart + blockIdx.x;
@@ -469,7 +697,10 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     }
     __syncthreads();
     if (tid == 0)
-        for (int i = 0; i < kRvMax + kRbMax; ++i) mbar_inval(&bars[i]);
+        for (int i = 0; i < kRvMax + kRbMax; ++i) {
+            mbar_inval(&full[i]);
+            mbar_inval(&empty[i]);
+        }
 }
 
 }  // namespace gm

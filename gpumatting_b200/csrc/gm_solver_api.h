@@ -9,7 +9,7 @@ namespace gm {
 // One operator source: band planes on the device, addressed as a 3-D tensor
 // {W, H, planes} with byte strides between rows and between planes.
 struct OpSource {
-    int kind;                 // OP_SYM (12 planes + gamma) or OP_REF25 (25 planes)
+    int kind;                 // OP_SYMD, OP_SYMI (12 planes) or OP_REF25 (25 planes)
     CUtensorMapDataType dt;   // element type of the planes
     int esize;                // bytes per element
     const void* base;         // plane 0, row 0
@@ -23,8 +23,10 @@ struct SolverSetup {
     OpSource lo;              // operator of the Krylov / Jacobi sweeps
     OpSource hi;              // true operator (replacement sweeps)
     bool mixed;               // keep the solution in FP64 between replacements
-    const float* gamma;       // OP_SYM: [H][gamma_pitch]
-    int gamma_pitch;
+    const float* xlo;         // OP_SYMD iteration operator: diagonal plane [H][xlo_pitch]
+    int xlo_pitch;
+    const float* xhi;         // OP_SYMI true operator: gamma plane [H][xhi_pitch]
+    int xhi_pitch;
     const float* b;           // [H][bpitch]
     int bpitch;
     const float* alpha_in;    // [H][alpha_pitch]

@@ -172,9 +172,13 @@ typedef struct gm_scribbles_s {
 } gm_scribbles;
 
 /* Symmetric Levin store: 12 planes of upper affinities
- * w_k(i) = -L(i, i + du_k + W dv_k), k = du + 5 dv in 1..12, the diagonal
- * being implicit (sum of the row's affinities, so rows of L sum to zero
- * exactly) plus gamma_i.  All planes are [H][pitch] on the device. */
+ * w_k(i) = -L(i, i + du_k + W dv_k), k = du + 5 dv in 1..12.  The Laplacian
+ * diagonal is not stored as a band: the true operator is
+ *   y_i = gamma_i x_i + sum_j w_ij (x_i - x_j)          (rows sum to gamma)
+ * and each set of planes carries the diagonal of exactly its own rounded
+ * weights, d_i = gamma_i + sum_j w_ij (summed in FP64, stored in FP32), so
+ * the low-precision operator y_i = d_i x_i - sum_j w_ij x_j keeps zero row
+ * sums too.  All planes are [H][pitch] on the device. */
 typedef struct gm_levin_store_s {
     int W, H, pitch;
     int precision;        /* element type of w                            */
@@ -182,6 +186,8 @@ typedef struct gm_levin_store_s {
     float* w32;           /* [12][H][pitch] FP32 affinities (true operator) */
     float* gamma;         /* [H][pitch] scribble weight                   */
     float* b;             /* [H][pitch] right-hand side gamma_i * s_i      */
+    float* d;             /* [H][pitch] gamma + row sum of w               */
+    float* d32;           /* [H][pitch] gamma + row sum of w32             */
     int owns;             /* set by gm_levin_store_alloc                  */
 } gm_levin_store;
 

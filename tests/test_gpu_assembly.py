@@ -38,6 +38,23 @@ def test_hostLevinLaplacian_dropin(case):
     assert np.array_equal(b, g["b"])
 
 
+def _row_diag(w, g, W, H):
+    """gamma + sum over the 24 stencil neighbours of the stored affinities."""
+    d = g.reshape(H, W).copy()
+    wp = w.reshape(12, H, W)
+    for k in range(1, 13):
+        dv = (k + 2) // 5
+        du = k - 5 * dv
+        d += wp[k - 1]
+        # lower neighbour (u - du, v - dv) holds w_k for the pair
+        sh = np.zeros((H, W))
+        v0, u0 = dv, max(0, du)
+        u1 = min(W, W + du)
+        sh[v0:, u0:u1] = wp[k - 1][: H - dv, u0 - du:u1 - du]
+        d += sh
+    return d.ravel()
+
+
 def _ulp_close(x, ref, dtype, ulps=1):
     r = ref.astype(dtype).astype(np.float64)
     x = x.astype(np.float64)
@@ -72,6 +89,11 @@ def test_fp64_assembly_matches_oracle(orc, W, H, prec, fmt):
     else:  # bf16: compare against the FP32 rounding at bf16 spacing
         assert np.all(np.abs(wl - w) <= np.abs(w) * 2.0 ** -8 + 1e-30)
     assert np.array_equal(st.planes("gamma")[:, :W].cpu().numpy().ravel(), g.astype(np.float32))
+    # diagonal planes: gamma + row sum of exactly the rounded weights
+    for dname, wp in (("d32", w32), ("d", wl)):
+        exp = _row_diag(wp.astype(np.float64), g, W, H).astype(np.float32)
+        got = st.planes(dname)[:, :W].cpu().numpy().ravel()
+        assert np.all(np.abs(got.astype(np.float64) - exp) <= np.spacing(np.abs(exp)) + 1e-30), dname
     assert np.array_equal(st.planes("b")[:, :W].cpu().numpy().ravel(), b.astype(np.float32))
     a25 = Lm.a.cpu().numpy()
     ref = bands25_f32(orc, w, g, W, H)

@@ -194,6 +194,21 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, uin
     return s_ok != 0;
 }
 
+// try_wait with a suspend-time hint: the warp parks in hardware until the
+// phase completes or about hint_ns pass, instead of spinning.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the mbarrier phase with a wall-clock limit; on expiry raises
 // GM_ERR_TIMEOUT in the grid barrier state and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, GridBarrier* gb,
@@ -202,8 +217,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     if (mbar_try_wait(bar, parity)) return true;
     uint64_t t0 = globaltimer_ns();
     unsigned spins = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) {
+    while (!mbar_try_wait_hint(bar, parity, 100000u)) {
+        if ((++spins & 15u) == 0 && globaltimer_ns() - t0 > limit_ns) {
             atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
             atomicExch(&gb->where, 2);
             return false;

@@ -241,8 +241,8 @@ template <class TLo, int OPLO, int OPHI, bool MIXED, int KIND>
 __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* smem, int u0, int v0, int v1,
                                           const KState& s, double (&part)[kNPart], Pipe& pp)
 {
-    const Layout& L = A.lay;
-    const KindLayout& K = L.k[KIND];
+    constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED);
+    constexpr KindLayout K = L.k[KIND];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nsteps = v1 - v0 + 4;
     const int nband = nsteps - 2;
@@ -329,7 +329,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     int bs0 = 0;      // band slot of step j-2 (valid from j = 2)
     int rj = 0;       // ring row of step j (j mod 6)
     int oj = 0;       // own ring row of step j (j mod 4)
-    const int Rb = K.Rb;
+    constexpr int Rb = K.Rb;
     for (int j = 0; j < nsteps; ++j) {
         const int Lr = v0 - 2 + j;
         {
@@ -375,7 +375,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                         *reinterpret_cast<float2*>(A.xacc[s.xsel] + gi) =
                             make_float2(fmaf(s.af, pv.x, xv.x), fmaf(s.af, pv.y, xv.y));
                     }
-                    part[0] += (double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y;
+                    part[0] += (double)fmaf(rn.x, rn.x, rn.y * rn.y);
                 } else if (in0) {
                     A.r[s.c ^ 1][gi] = rn.x;
                     A.p[s.c ^ 1][gi] = pn.x;
@@ -463,9 +463,10 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                     const float2 rn = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
                     if (in1) {
                         *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go) = q;
-                        part[1] += (double)X[2][2] * (double)q.x + (double)X[2][3] * (double)q.y;
-                        part[2] += (double)rn.x * (double)q.x + (double)rn.y * (double)q.y;
-                        part[3] += (double)q.x * (double)q.x + (double)q.y * (double)q.y;
+                        // pair sums in FP32, accumulated in FP64
+                        part[1] += (double)fmaf(X[2][2], q.x, X[2][3] * q.y);
+                        part[2] += (double)fmaf(rn.x, q.x, rn.y * q.y);
+                        part[3] += (double)fmaf(q.x, q.x, q.y * q.y);
                     } else {
                         A.q[s.c ^ 1][go] = q.x;
                         part[1] += (double)X[2][2] * (double)q.x;
@@ -534,7 +535,7 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;
-    const Layout& L = A.lay;
+    constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     double* red = reinterpret_cast<double*>(smem + L.red_off);

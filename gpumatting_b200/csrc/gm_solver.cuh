@@ -22,8 +22,9 @@ constexpr int kRvMax = 16;                       // vector ring slots
 constexpr int kRbMax = 16;                       // band ring slots
 constexpr int kNPart = 4;                        // FP64 partial sums per CTA per sweep
 
-// Shared-memory carve of one sweep kind (bytes from the start of dynamic
-// shared memory; every TMA destination is 128-byte aligned).
+// Shared-memory carve of one sweep kind.  Everything here is a compile-time
+// function of the operator types, so the hot loop indexes rings with
+// constants; the host uses the same functions to size the launch.
 struct KindLayout {
     int D;          // prefetch distance in rows
     int Rv, Rb;     // ring slots
@@ -35,13 +36,72 @@ struct KindLayout {
     int pstride;    // bytes between planes inside a band slot (= kBox * elem)
     int xoff;       // offset of the extra plane row (diagonal or gamma), -1 none
     int bbytes;     // TMA bytes of one band row (planes + extra)
-    int band_life;  // steps a band row stays in use after its first use (2 sym, 0 ref25)
 };
+
+__host__ __device__ constexpr int a128(int x) { return (x + 127) & ~127; }
+
+// Vector rows per step: Krylov r, q, p, x increment; replacement base (FP64,
+// mixed only), x increment, p, b; Jacobi x, -, -, b.
+__host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize, bool mixed, int D)
+{
+    KindLayout K{};
+    const int vb4 = kBox * 4;
+    int vb[4] = {0, 0, 0, 0};
+    if (kind == KIND_KRYLOV) { vb[0] = vb4; vb[1] = vb4; vb[2] = vb4; vb[3] = vb4; }
+    else if (kind == KIND_REPLACE) { vb[0] = mixed ? 2 * vb4 : 0; vb[1] = vb4; vb[2] = vb4; vb[3] = vb4; }
+    else { vb[0] = vb4; vb[3] = vb4; }
+    int off = 0;
+    for (int i = 0; i < 4; ++i) {
+        K.voff[i] = off;
+        K.vbytes[i] = vb[i];
+        off += a128(vb[i]);
+    }
+    K.vslot = off;
+    const bool sym = op != OP_REF25;
+    K.planes = sym ? 12 : 25;
+    K.pstride = kBox * esize;
+    const int pbytes = K.planes * K.pstride;
+    K.xoff = sym ? a128(pbytes) : -1;
+    K.bbytes = pbytes + (sym ? kBox * 4 : 0);
+    K.bslot = sym ? a128(K.xoff + kBox * 4) : a128(pbytes);
+    K.D = D;
+    K.Rv = D + 1;
+    K.Rb = D + (sym ? 3 : 1);
+    return K;
+}
+
+// Prefetch depths: Krylov sweeps are the hot path; replacement and Jacobi
+// sweeps (rare, FP32 planes) run shallower so three CTAs fit per SM.
+__host__ __device__ constexpr int depth_of(int kind, int oplo) { return kind == KIND_KRYLOV ? (oplo == OP_REF25 ? 3 : 4) : 1; }
 
 struct Layout {
     int vring_off, bring_off, pring_off, rring_off, full_off, empty_off, red_off, total;
     KindLayout k[NKIND];
 };
+
+__host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
+
+__host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int ophi, bool mixed)
+{
+    Layout L{};
+    L.k[KIND_KRYLOV] = kind_layout(KIND_KRYLOV, oplo, esize_lo, mixed, depth_of(KIND_KRYLOV, oplo));
+    L.k[KIND_REPLACE] = kind_layout(KIND_REPLACE, ophi, 4, mixed, depth_of(KIND_REPLACE, oplo));
+    L.k[KIND_JACOBI] = kind_layout(KIND_JACOBI, ophi, 4, mixed, depth_of(KIND_JACOBI, oplo));
+    int vcap = 0, bcap = 0;
+    for (int k = 0; k < NKIND; ++k) {
+        vcap = imax(vcap, L.k[k].Rv * L.k[k].vslot);
+        bcap = imax(bcap, L.k[k].Rb * L.k[k].bslot);
+    }
+    L.vring_off = 0;
+    L.bring_off = a128(vcap);
+    L.pring_off = L.bring_off + a128(bcap);
+    L.rring_off = L.pring_off + a128(kConsumers * 6 * kRingCols * 8);
+    L.full_off = L.rring_off + a128(kConsumers * 4 * kWarpCols * 4);
+    L.empty_off = L.full_off + a128((kRvMax + kRbMax) * 8);
+    L.red_off = L.empty_off + a128((kRvMax + kRbMax) * 8);
+    L.total = L.red_off + a128(32 * kNPart * 8 + 16);
+    return L;
+}
 
 struct SolverOut {
     int status;
@@ -71,7 +131,6 @@ struct SolverArgs {
     int P;                    // pitch (elements) of the work vectors
     int W, H;
     int nstrips, nseg, nunits;
-    Layout lay;
     double* partials;         // [2][kNPart][grid]
     GridBarrier* gb;
     SolverOut* out;

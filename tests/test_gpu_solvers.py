@@ -209,4 +209,4 @@ def test_bad_arguments():
 
     alpha = torch.zeros((16, 16), device="cuda")
     with pytest.raises(L.GmError):
-        st.solve(alpha, "cg", strip_width=4)
+        st.solve(alpha, "cg", max_iters=-1)

@@ -97,37 +97,40 @@ __device__ __forceinline__ const T* plane(const unsigned char* slot, int k, int 
 // X[d][m]: operand at row v + d - 2, local column 2*lane + m (output pixel e
 // sits at m = 2 + e).  brow[d]: band slot of row v - d.
 template <class T, int K>
-__device__ __forceinline__ void symd_term(float& y0, float& y1, const float (&X)[5][6],
+__device__ __forceinline__ void symd_term(float2& yu, float2& yl, const float (&X)[5][6],
                                           const unsigned char* const (&brow)[3], int pstride, int c)
 {
     constexpr int du = sym_du(K), dv = sym_dv(K);
     const float2 wu = ld2(plane<T>(brow[0], K - 1, pstride), c);
-    y0 = fmaf(-wu.x, X[2 + dv][2 + du], y0);
-    y1 = fmaf(-wu.y, X[2 + dv][3 + du], y1);
+    yu.x = fmaf(-wu.x, X[2 + dv][2 + du], yu.x);
+    yu.y = fmaf(-wu.y, X[2 + dv][3 + du], yu.y);
     const float2 wl = ld2s<du>(plane<T>(brow[dv], K - 1, pstride), c - du);
-    y0 = fmaf(-wl.x, X[2 - dv][2 - du], y0);
-    y1 = fmaf(-wl.y, X[2 - dv][3 - du], y1);
+    yl.x = fmaf(-wl.x, X[2 - dv][2 - du], yl.x);
+    yl.y = fmaf(-wl.y, X[2 - dv][3 - du], yl.y);
 }
 
+// Four independent accumulation chains per pixel (upper/lower x two halves
+// of the bands) keep the FMA dependency chains short.
 template <class T>
 __device__ __forceinline__ float2 symd_apply(const float (&X)[5][6], const unsigned char* const (&brow)[3], int pstride,
                                              int xoff, int c)
 {
     const float2 dg = ld2(reinterpret_cast<const float*>(brow[0] + xoff), c);
-    float y0 = dg.x * X[2][2], y1 = dg.y * X[2][3];
-    symd_term<T, 1>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 2>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 3>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 4>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 5>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 6>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 7>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 8>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 9>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 10>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 11>(y0, y1, X, brow, pstride, c);
-    symd_term<T, 12>(y0, y1, X, brow, pstride, c);
-    return make_float2(y0, y1);
+    float2 a = make_float2(dg.x * X[2][2], dg.y * X[2][3]);
+    float2 b = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
+    symd_term<T, 1>(a, b, X, brow, pstride, c);
+    symd_term<T, 2>(e, f, X, brow, pstride, c);
+    symd_term<T, 3>(a, b, X, brow, pstride, c);
+    symd_term<T, 4>(e, f, X, brow, pstride, c);
+    symd_term<T, 5>(a, b, X, brow, pstride, c);
+    symd_term<T, 6>(e, f, X, brow, pstride, c);
+    symd_term<T, 7>(a, b, X, brow, pstride, c);
+    symd_term<T, 8>(e, f, X, brow, pstride, c);
+    symd_term<T, 9>(a, b, X, brow, pstride, c);
+    symd_term<T, 10>(e, f, X, brow, pstride, c);
+    symd_term<T, 11>(a, b, X, brow, pstride, c);
+    symd_term<T, 12>(e, f, X, brow, pstride, c);
+    return make_float2((a.x + b.x) + (e.x + f.x), (a.y + b.y) + (e.y + f.y));
 }
 
 // True operator, implicit diagonal, accumulation type V (float or double);
@@ -174,19 +177,20 @@ template <class V>
 __device__ __forceinline__ void ref25_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
                                             const unsigned char* b0, int pstride, int c)
 {
-    y0 = 0;
-    y1 = 0;
+    V s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0};  // three chains per pixel
 #pragma unroll
     for (int j = 0; j < 25; ++j) {
         const int du = j % 5 - 2, dv = j / 5 - 2;
         const float2 a = ld2(plane<float>(b0, j, pstride), c);
-        y0 += (V)a.x * X[2 + dv][2 + du];
-        y1 += (V)a.y * X[2 + dv][3 + du];
+        s0[j % 3] += (V)a.x * X[2 + dv][2 + du];
+        s1[j % 3] += (V)a.y * X[2 + dv][3 + du];
         if (j == 12) {
             d0 = (V)a.x;
             d1 = (V)a.y;
         }
     }
+    y0 = (s0[0] + s0[1]) + s0[2];
+    y1 = (s1[0] + s1[1]) + s1[2];
 }
 
 struct KState {

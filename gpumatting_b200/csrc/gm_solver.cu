@@ -49,6 +49,8 @@
 //
 // Every wait (grid barrier, ring slot) has a wall-clock limit; on expiry the
 // kernel records GM_ERR_TIMEOUT and all CTAs leave their loops.
+#include <type_traits>
+
 #include "gm_solver.cuh"
 
 namespace gm {
@@ -94,96 +96,100 @@ __device__ __forceinline__ const T* plane(const unsigned char* slot, int k, int 
 }
 
 // ---- operators on two adjacent output pixels (smem column c, c+1) ----
-// X[d][m]: operand at row v + d - 2, local column 2*lane + m (output pixel e
-// sits at m = 2 + e).  brow[d]: band slot of row v - d.
-template <class T, int K>
-__device__ __forceinline__ void symd_term(float2& yu, float2& yl, const float (&X)[5][6],
-                                          const unsigned char* const (&brow)[3], int pstride, int c)
+// X[d][m]: operand at row vbase + d - 2, local column 2*lane + m (output
+// pixel e sits at m = 2 + e); the output row is vbase + RO, so rows
+// RO..RO+4 of X are its stencil rows.  brow[d]: band slot of row v - d.
+template <class T, int K, int RO>
+__device__ __forceinline__ void symd_term(float2& yu, float2& yl, const float (&X)[6][6],
+                                          const unsigned char* const (&brow)[3], int c)
 {
     constexpr int du = sym_du(K), dv = sym_dv(K);
+    constexpr int pstride = kBox * (int)sizeof(T);
     const float2 wu = ld2(plane<T>(brow[0], K - 1, pstride), c);
-    yu.x = fmaf(-wu.x, X[2 + dv][2 + du], yu.x);
-    yu.y = fmaf(-wu.y, X[2 + dv][3 + du], yu.y);
+    yu.x = fmaf(-wu.x, X[RO + 2 + dv][2 + du], yu.x);
+    yu.y = fmaf(-wu.y, X[RO + 2 + dv][3 + du], yu.y);
     const float2 wl = ld2s<du>(plane<T>(brow[dv], K - 1, pstride), c - du);
-    yl.x = fmaf(-wl.x, X[2 - dv][2 - du], yl.x);
-    yl.y = fmaf(-wl.y, X[2 - dv][3 - du], yl.y);
+    yl.x = fmaf(-wl.x, X[RO + 2 - dv][2 - du], yl.x);
+    yl.y = fmaf(-wl.y, X[RO + 2 - dv][3 - du], yl.y);
 }
 
 // Four independent accumulation chains per pixel (upper/lower x two halves
 // of the bands) keep the FMA dependency chains short.
-template <class T>
-__device__ __forceinline__ float2 symd_apply(const float (&X)[5][6], const unsigned char* const (&brow)[3], int pstride,
-                                             int xoff, int c)
+template <class T, int RO>
+__device__ __forceinline__ float2 symd_apply(const float (&X)[6][6], const unsigned char* const (&brow)[3], int xoff,
+                                             int c)
 {
     const float2 dg = ld2(reinterpret_cast<const float*>(brow[0] + xoff), c);
-    float2 a = make_float2(dg.x * X[2][2], dg.y * X[2][3]);
+    float2 a = make_float2(dg.x * X[RO + 2][2], dg.y * X[RO + 2][3]);
     float2 b = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
-    symd_term<T, 1>(a, b, X, brow, pstride, c);
-    symd_term<T, 2>(e, f, X, brow, pstride, c);
-    symd_term<T, 3>(a, b, X, brow, pstride, c);
-    symd_term<T, 4>(e, f, X, brow, pstride, c);
-    symd_term<T, 5>(a, b, X, brow, pstride, c);
-    symd_term<T, 6>(e, f, X, brow, pstride, c);
-    symd_term<T, 7>(a, b, X, brow, pstride, c);
-    symd_term<T, 8>(e, f, X, brow, pstride, c);
-    symd_term<T, 9>(a, b, X, brow, pstride, c);
-    symd_term<T, 10>(e, f, X, brow, pstride, c);
-    symd_term<T, 11>(a, b, X, brow, pstride, c);
-    symd_term<T, 12>(e, f, X, brow, pstride, c);
+    symd_term<T, 1, RO>(a, b, X, brow, c);
+    symd_term<T, 2, RO>(e, f, X, brow, c);
+    symd_term<T, 3, RO>(a, b, X, brow, c);
+    symd_term<T, 4, RO>(e, f, X, brow, c);
+    symd_term<T, 5, RO>(a, b, X, brow, c);
+    symd_term<T, 6, RO>(e, f, X, brow, c);
+    symd_term<T, 7, RO>(a, b, X, brow, c);
+    symd_term<T, 8, RO>(e, f, X, brow, c);
+    symd_term<T, 9, RO>(a, b, X, brow, c);
+    symd_term<T, 10, RO>(e, f, X, brow, c);
+    symd_term<T, 11, RO>(a, b, X, brow, c);
+    symd_term<T, 12, RO>(e, f, X, brow, c);
     return make_float2((a.x + b.x) + (e.x + f.x), (a.y + b.y) + (e.y + f.y));
 }
 
 // True operator, implicit diagonal, accumulation type V (float or double);
 // also returns the diagonal gamma + sum w (for Jacobi).
-template <class V, int K>
-__device__ __forceinline__ void symi_term(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
-                                          const unsigned char* const (&brow)[3], int pstride, int c)
+template <class V, int K, int RO>
+__device__ __forceinline__ void symi_term(V& y0, V& y1, V& d0, V& d1, const V (&X)[6][6],
+                                          const unsigned char* const (&brow)[3], int c)
 {
     constexpr int du = sym_du(K), dv = sym_dv(K);
+    constexpr int pstride = kBox * 4;
     const float2 wu = ld2(plane<float>(brow[0], K - 1, pstride), c);
     const float2 wl = ld2s<du>(plane<float>(brow[dv], K - 1, pstride), c - du);
-    y0 += (V)wu.x * (X[2][2] - X[2 + dv][2 + du]) + (V)wl.x * (X[2][2] - X[2 - dv][2 - du]);
-    y1 += (V)wu.y * (X[2][3] - X[2 + dv][3 + du]) + (V)wl.y * (X[2][3] - X[2 - dv][3 - du]);
+    y0 += (V)wu.x * (X[RO + 2][2] - X[RO + 2 + dv][2 + du]) + (V)wl.x * (X[RO + 2][2] - X[RO + 2 - dv][2 - du]);
+    y1 += (V)wu.y * (X[RO + 2][3] - X[RO + 2 + dv][3 + du]) + (V)wl.y * (X[RO + 2][3] - X[RO + 2 - dv][3 - du]);
     d0 += (V)wu.x + (V)wl.x;
     d1 += (V)wu.y + (V)wl.y;
 }
 
-template <class V>
-__device__ __forceinline__ void symi_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
-                                           const unsigned char* const (&brow)[3], int pstride, int xoff, int c)
+template <class V, int RO>
+__device__ __forceinline__ void symi_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[6][6],
+                                           const unsigned char* const (&brow)[3], int xoff, int c)
 {
     const float2 g = ld2(reinterpret_cast<const float*>(brow[0] + xoff), c);
-    y0 = (V)g.x * X[2][2];
-    y1 = (V)g.y * X[2][3];
+    y0 = (V)g.x * X[RO + 2][2];
+    y1 = (V)g.y * X[RO + 2][3];
     d0 = (V)g.x;
     d1 = (V)g.y;
-    symi_term<V, 1>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 2>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 3>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 4>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 5>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 6>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 7>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 8>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 9>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 10>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 11>(y0, y1, d0, d1, X, brow, pstride, c);
-    symi_term<V, 12>(y0, y1, d0, d1, X, brow, pstride, c);
+    symi_term<V, 1, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 2, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 3, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 4, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 5, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 6, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 7, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 8, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 9, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 10, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 11, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 12, RO>(y0, y1, d0, d1, X, brow, c);
 }
 
 // Reference layout: y = sum_j a_j x(u+du_j, v+dv_j), band j = 12 + du + 5 dv,
 // in band order (BandedMatrix.cu:172-173); d = a_12.
-template <class V>
-__device__ __forceinline__ void ref25_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[5][6],
-                                            const unsigned char* b0, int pstride, int c)
+template <class V, int RO>
+__device__ __forceinline__ void ref25_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[6][6],
+                                            const unsigned char* b0, int c)
 {
+    constexpr int pstride = kBox * 4;
     V s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0};  // three chains per pixel
 #pragma unroll
     for (int j = 0; j < 25; ++j) {
         const int du = j % 5 - 2, dv = j / 5 - 2;
         const float2 a = ld2(plane<float>(b0, j, pstride), c);
-        s0[j % 3] += (V)a.x * X[2 + dv][2 + du];
-        s1[j % 3] += (V)a.y * X[2 + dv][3 + du];
+        s0[j % 3] += (V)a.x * X[RO + 2 + dv][2 + du];
+        s1[j % 3] += (V)a.y * X[RO + 2 + dv][3 + du];
         if (j == 12) {
             d0 = (V)a.x;
             d1 = (V)a.y;
@@ -217,15 +223,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Rows vbase-2 .. vbase+3 of the operand sit in ring rows r0, r0+1, ...
+// (mod 8); columns lc0 .. lc0+5.
 template <class V>
-__device__ __forceinline__ void load_rows(V (&X)[5][6], const V* ring, int r0, int lc0)
+__device__ __forceinline__ void load_rows(V (&X)[6][6], const V* ring, int r0, int lc0)
 {
-    // rows v-2..v+2 sit in ring rows r0, r0+1, ... (mod 6); columns lc0..lc0+5
 #pragma unroll
-    for (int d = 0; d < 5; ++d) {
-        int r = r0 + d;
-        r = r >= 6 ? r - 6 : r;
-        const V* row = ring + r * kRingCols + lc0;
+    for (int d = 0; d < 6; ++d) {
+        const V* row = ring + ((r0 + d) & 7) * kRingCols + lc0;
 #pragma unroll
         for (int m = 0; m < 6; m += 2) {
             if constexpr (sizeof(V) == 4) {
@@ -315,6 +320,9 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     }
 
     // -------------------------------- consumers --------------------------------
+    // Rows are consumed in super-steps of two: phase A of steps j and j+1
+    // (combine the incoming rows into the operand ring), one __syncwarp, then
+    // phase B of both output rows from one shared 6-row operand window.
     const int w = warp;
     const int c = 8 + kWarpCols * w + 2 * lane;        // smem column of this lane's pixel pair
     const int lc0 = 2 * lane;                          // first operand column (local ring index)
@@ -324,17 +332,21 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     const bool has_x = lane < 2;
     const int cx = lane == 0 ? 6 + kWarpCols * w : 8 + kWarpCols * w + kWarpCols;
     const int lcx = lane == 0 ? 0 : kRingCols - 2;
-    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * 6 * kRingCols * 2;
-    double* ring_d = reinterpret_cast<double*>(smem + L.pring_off) + w * 6 * kRingCols;
+    using RingT = std::conditional_t<MIXED, double, float>;  // replacement operand ring element
+    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * 8 * kRingCols * (MIXED ? 2 : 1);
+    RingT* ring_d = reinterpret_cast<RingT*>(smem + L.pring_off) + w * 8 * kRingCols;
     float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * 4 * kWarpCols;  // r or b, own columns
     const int P = A.P;
-
-    int vs = 0;       // vector slot of step j
-    int bs0 = 0;      // band slot of step j-2 (valid from j = 2)
-    int rj = 0;       // ring row of step j (j mod 6)
-    int oj = 0;       // own ring row of step j (j mod 4)
     constexpr int Rb = K.Rb;
-    for (int j = 0; j < nsteps; ++j) {
+
+    int vs = 0;    // vector slot of the next step
+    int bsn = 0;   // band slot of the next band step to wait for
+    int bwait = 0; // next band step to wait for
+    int brel = 0;  // next band step to release
+    int brel_s = 0;
+
+    // phase A of step j into operand ring row (j & 7) and own ring row (j & 3)
+    auto phase_a = [&](int j) {
         const int Lr = v0 - 2 + j;
         {
             const uint32_t bit = 1u << vs;
@@ -345,7 +357,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
         const unsigned char* vsp = vring + vs * K.vslot;
         const bool own_row = Lr >= v0 && Lr < v1;
         const size_t gi = (size_t)(own_row ? Lr : 0) * P + u;
-        // ---------------- phase A: combine the incoming row ----------------
+        const int rr = j & 7, orow = j & 3;
         if (KIND == KIND_KRYLOV) {
             const float* vr = reinterpret_cast<const float*>(vsp + K.voff[0]);
             const float* vq = reinterpret_cast<const float*>(vsp + K.voff[1]);
@@ -364,13 +376,13 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
             };
             float2 rn, pv;
             const float2 pn = combine(c, rn, pv);
-            *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lc0 + 2) = pn;
+            *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lc0 + 2) = pn;
             if (has_x) {
                 float2 rx, px;
-                *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lcx) = combine(cx, rx, px);
+                *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lcx) = combine(cx, rx, px);
             }
             if (own_row) {
-                *reinterpret_cast<float2*>(own_ring + oj * kWarpCols + lc0) = rn;
+                *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = rn;
                 if (in1) {
                     *reinterpret_cast<float2*>(A.r[s.c ^ 1] + gi) = rn;
                     *reinterpret_cast<float2*>(A.p[s.c ^ 1] + gi) = pn;
@@ -406,10 +418,18 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                 return xf;
             };
             const double2 xf = fold(c);
-            *reinterpret_cast<double2*>(ring_d + rj * kRingCols + lc0 + 2) = xf;
-            if (has_x) *reinterpret_cast<double2*>(ring_d + rj * kRingCols + lcx) = fold(cx);
+            if constexpr (MIXED) {
+                *reinterpret_cast<double2*>(ring_d + rr * kRingCols + lc0 + 2) = xf;
+                if (has_x) *reinterpret_cast<double2*>(ring_d + rr * kRingCols + lcx) = fold(cx);
+            } else {
+                *reinterpret_cast<float2*>(ring_d + rr * kRingCols + lc0 + 2) = make_float2((float)xf.x, (float)xf.y);
+                if (has_x) {
+                    const double2 xx = fold(cx);
+                    *reinterpret_cast<float2*>(ring_d + rr * kRingCols + lcx) = make_float2((float)xx.x, (float)xx.y);
+                }
+            }
             if (own_row) {
-                *reinterpret_cast<float2*>(own_ring + oj * kWarpCols + lc0) = ld2(vb, c);
+                *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = ld2(vb, c);
                 if (in1) {
                     if (MIXED) {
                         *reinterpret_cast<double2*>(A.base[s.xsel ^ 1] + gi) = xf;
@@ -429,109 +449,173 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
         } else {  // Jacobi
             const float* vx = reinterpret_cast<const float*>(vsp + K.voff[0]);
             const float* vb = reinterpret_cast<const float*>(vsp + K.voff[3]);
-            *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lc0 + 2) = ld2(vx, c);
-            if (has_x) *reinterpret_cast<float2*>(ring_f + rj * kRingCols + lcx) = ld2(vx, cx);
-            if (own_row) *reinterpret_cast<float2*>(own_ring + oj * kWarpCols + lc0) = ld2(vb, c);
+            *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lc0 + 2) = ld2(vx, c);
+            if (has_x) *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lcx) = ld2(vx, cx);
+            if (own_row) *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = ld2(vb, c);
+        }
+    };
+    auto wait_band = [&]() {
+        const uint32_t bit = 1u << bsn;
+        if (!*s_abort && !mbar_wait_bounded(&full[kRvMax + bsn], (pp.full_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
+            *s_abort = 1;
+        pp.full_b ^= bit;
+        bsn = ring_next(bsn, Rb);
+        ++bwait;
+    };
+    auto release_bands_to = [&](int m_end) {  // release band steps [brel, m_end)
+        for (; brel < m_end; ++brel) {
+            if (lane == 0) mbar_arrive(&empty[kRvMax + brel_s]);
+            brel_s = ring_next(brel_s, Rb);
+        }
+    };
+    // band slot of band step m, given that bsn is the slot of step bwait
+    auto bslot_of = [&](int m) {
+        int sl = bsn - (bwait - m);
+        while (sl < 0) sl += Rb;
+        return sl;
+    };
+
+    for (int j = 0; j < nsteps; j += 2) {
+        const bool two = j + 1 < nsteps;
+        phase_a(j);
+        const int vs0 = vs;
+        vs = ring_next(vs, K.Rv);
+        if (two) {
+            phase_a(j + 1);
+            vs = ring_next(vs, K.Rv);
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[vs]);
-        vs = ring_next(vs, K.Rv);
-        if (j >= 2) {
-            if (j > 2) bs0 = ring_next(bs0, Rb);
-            const uint32_t bit = 1u << bs0;
-            if (!*s_abort && !mbar_wait_bounded(&full[kRvMax + bs0], (pp.full_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
-                *s_abort = 1;
-            pp.full_b ^= bit;
+        if (lane == 0) {
+            mbar_arrive(&empty[vs0]);
+            if (two) mbar_arrive(&empty[ring_next(vs0, K.Rv)]);
         }
+        // band steps up to (last step of this super-step) - 2
+        const int mneed = (two ? j + 1 : j) - 2;
+        while (bwait <= mneed) wait_band();
         if (j >= 4) {
-            // ---------------- phase B: stencil on output row v ----------------
-            const int v = Lr - 2;
-            const int b1 = ring_prev(bs0, Rb), b2 = ring_prev(b1, Rb);
-            const unsigned char* brow[3] = {bring + bs0 * K.bslot, bring + b1 * K.bslot, bring + b2 * K.bslot};
-            int r0 = rj + 2;  // ring row of step j-4 = (j + 2) mod 6
-            r0 = r0 >= 6 ? r0 - 6 : r0;
-            int o2 = oj + 2;  // own ring row of step j-2
-            o2 = o2 >= 4 ? o2 - 4 : o2;
+            // ---------------- phase B: output rows v and v+1 ----------------
+            const int v = v0 - 4 + j;
+            const bool second = two && v + 1 < v1;
+            const unsigned char* bA[3] = {bring + bslot_of(j - 2) * K.bslot, bring + bslot_of(j - 3) * K.bslot,
+                                          bring + bslot_of(j - 4) * K.bslot};
+            const unsigned char* bB[3] = {bring + bslot_of(j - 1) * K.bslot, bA[0], bA[1]};
+            const int r0 = (j - 4) & 7;   // ring row of operand row v - 2
+            const int o0 = (j - 2) & 3;   // own ring row of output row v
+            const int o1 = (j - 1) & 3;
             const size_t go = (size_t)v * P + u;
             if (in0) {
                 if (KIND == KIND_KRYLOV) {
-                    float X[5][6];
+                    float X[6][6];
                     load_rows<float>(X, ring_f, r0, lc0);
-                    float2 q;
+                    float2 q0, q1 = make_float2(0.f, 0.f);
                     if (OPLO == OP_SYMD) {
-                        q = symd_apply<TLo>(X, brow, K.pstride, K.xoff, c);
+                        q0 = symd_apply<TLo, 0>(X, bA, K.xoff, c);
+                        if (second) q1 = symd_apply<TLo, 1>(X, bB, K.xoff, c);
                     } else {
                         float d0, d1;
-                        ref25_apply<float>(q.x, q.y, d0, d1, X, brow[0], K.pstride, c);
+                        ref25_apply<float, 0>(q0.x, q0.y, d0, d1, X, bA[0], c);
+                        if (second) ref25_apply<float, 1>(q1.x, q1.y, d0, d1, X, bB[0], c);
                     }
-                    const float2 rn = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
+                    const float2 rn0 = *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0);
+                    const float2 rn1 = *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0);
                     if (in1) {
-                        *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go) = q;
-                        // pair sums in FP32, accumulated in FP64
-                        part[1] += (double)fmaf(X[2][2], q.x, X[2][3] * q.y);
-                        part[2] += (double)fmaf(rn.x, q.x, rn.y * q.y);
-                        part[3] += (double)fmaf(q.x, q.x, q.y * q.y);
+                        *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go) = q0;
+                        float spq = fmaf(X[2][2], q0.x, X[2][3] * q0.y);
+                        float srq = fmaf(rn0.x, q0.x, rn0.y * q0.y);
+                        float sqq = fmaf(q0.x, q0.x, q0.y * q0.y);
+                        if (second) {
+                            *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go + P) = q1;
+                            part[1] += (double)fmaf(X[3][2], q1.x, X[3][3] * q1.y);
+                            part[2] += (double)fmaf(rn1.x, q1.x, rn1.y * q1.y);
+                            part[3] += (double)fmaf(q1.x, q1.x, q1.y * q1.y);
+                        }
+                        part[1] += (double)spq;
+                        part[2] += (double)srq;
+                        part[3] += (double)sqq;
                     } else {
-                        A.q[s.c ^ 1][go] = q.x;
-                        part[1] += (double)X[2][2] * (double)q.x;
-                        part[2] += (double)rn.x * (double)q.x;
-                        part[3] += (double)q.x * (double)q.x;
+                        A.q[s.c ^ 1][go] = q0.x;
+                        part[1] += (double)X[2][2] * (double)q0.x;
+                        part[2] += (double)rn0.x * (double)q0.x;
+                        part[3] += (double)q0.x * (double)q0.x;
+                        if (second) {
+                            A.q[s.c ^ 1][go + P] = q1.x;
+                            part[1] += (double)X[3][2] * (double)q1.x;
+                            part[2] += (double)rn1.x * (double)q1.x;
+                            part[3] += (double)q1.x * (double)q1.x;
+                        }
                     }
                 } else if (KIND == KIND_REPLACE) {
-                    double X[5][6];
-                    load_rows<double>(X, ring_d, r0, lc0);
+                    double X[6][6];
+                    if constexpr (MIXED) {
+                        load_rows<double>(X, ring_d, r0, lc0);
+                    } else {
+                        float Xf[6][6];
+                        load_rows<float>(Xf, ring_d, r0, lc0);
+#pragma unroll
+                        for (int a = 0; a < 6; ++a)
+#pragma unroll
+                            for (int b2 = 0; b2 < 6; ++b2) X[a][b2] = (double)Xf[a][b2];
+                    }
+                    auto rep_row = [&](double y0, double y1, const float2 bv, size_t g, int vr, int ro) {
+                        const float r0f = (float)((double)bv.x - y0), r1f = (float)((double)bv.y - y1);
+                        float* ao = A.alpha_out + (size_t)vr * A.alpha_pitch + u;
+                        ao[0] = (float)X[ro + 2][2];
+                        A.r[s.c][g] = r0f;
+                        part[0] += (double)r0f * (double)r0f;
+                        part[1] += (double)bv.x * (double)bv.x;
+                        if (in1) {
+                            ao[1] = (float)X[ro + 2][3];
+                            A.r[s.c][g + 1] = r1f;
+                            part[0] += (double)r1f * (double)r1f;
+                            part[1] += (double)bv.y * (double)bv.y;
+                        }
+                    };
                     double y0, y1, d0, d1;
-                    if (OPHI == OP_REF25) ref25_apply<double>(y0, y1, d0, d1, X, brow[0], K.pstride, c);
-                    else symi_apply<double>(y0, y1, d0, d1, X, brow, K.pstride, K.xoff, c);
-                    const float2 bv = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
-                    const float r0f = (float)((double)bv.x - y0), r1f = (float)((double)bv.y - y1);
-                    float* ao = A.alpha_out + (size_t)v * A.alpha_pitch + u;
-                    ao[0] = (float)X[2][2];
-                    A.r[s.c][go] = r0f;
-                    part[0] += (double)r0f * (double)r0f;
-                    part[1] += (double)bv.x * (double)bv.x;
-                    if (in1) {
-                        ao[1] = (float)X[2][3];
-                        A.r[s.c][go + 1] = r1f;
-                        part[0] += (double)r1f * (double)r1f;
-                        part[1] += (double)bv.y * (double)bv.y;
+                    if (OPHI == OP_REF25) ref25_apply<double, 0>(y0, y1, d0, d1, X, bA[0], c);
+                    else symi_apply<double, 0>(y0, y1, d0, d1, X, bA, K.xoff, c);
+                    rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, v, 0);
+                    if (second) {
+                        if (OPHI == OP_REF25) ref25_apply<double, 1>(y0, y1, d0, d1, X, bB[0], c);
+                        else symi_apply<double, 1>(y0, y1, d0, d1, X, bB, K.xoff, c);
+                        rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0), go + P,
+                                v + 1, 1);
                     }
                 } else {  // Jacobi
-                    float X[5][6];
+                    float X[6][6];
                     load_rows<float>(X, ring_f, r0, lc0);
+                    auto jac_row = [&](float y0, float y1, float d0, float d1, const float2 bv, size_t g, int ro) {
+                        const float rv0 = bv.x - y0, rv1 = bv.y - y1;
+                        A.xacc[s.xsel ^ 1][g] = X[ro + 2][2] + A.omega * rv0 / d0;
+                        part[0] += (double)rv0 * (double)rv0;
+                        part[1] += (double)bv.x * (double)bv.x;
+                        if (in1) {
+                            A.xacc[s.xsel ^ 1][g + 1] = X[ro + 2][3] + A.omega * rv1 / d1;
+                            part[0] += (double)rv1 * (double)rv1;
+                            part[1] += (double)bv.y * (double)bv.y;
+                        }
+                    };
                     float y0, y1, d0, d1;
-                    if (OPHI == OP_REF25) ref25_apply<float>(y0, y1, d0, d1, X, brow[0], K.pstride, c);
-                    else symi_apply<float>(y0, y1, d0, d1, X, brow, K.pstride, K.xoff, c);
-                    const float2 bv = *reinterpret_cast<const float2*>(own_ring + o2 * kWarpCols + lc0);
-                    const float rv0 = bv.x - y0, rv1 = bv.y - y1;
-                    A.xacc[s.xsel ^ 1][go] = X[2][2] + A.omega * rv0 / d0;
-                    part[0] += (double)rv0 * (double)rv0;
-                    part[1] += (double)bv.x * (double)bv.x;
-                    if (in1) {
-                        A.xacc[s.xsel ^ 1][go + 1] = X[2][3] + A.omega * rv1 / d1;
-                        part[0] += (double)rv1 * (double)rv1;
-                        part[1] += (double)bv.y * (double)bv.y;
+                    if (OPHI == OP_REF25) ref25_apply<float, 0>(y0, y1, d0, d1, X, bA[0], c);
+                    else symi_apply<float, 0>(y0, y1, d0, d1, X, bA, K.xoff, c);
+                    jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, 0);
+                    if (second) {
+                        if (OPHI == OP_REF25) ref25_apply<float, 1>(y0, y1, d0, d1, X, bB[0], c);
+                        else symi_apply<float, 1>(y0, y1, d0, d1, X, bB, K.xoff, c);
+                        jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0),
+                                go + P, 1);
                     }
                 }
             }
             __syncwarp();
-            // release the band row whose last use this was
-            if (lane == 0) mbar_arrive(&empty[kRvMax + (kSymBand ? b2 : bs0)]);
-        } else if (j >= 2 && !kSymBand) {
+            // band rows whose last use was this super-step
+            release_bands_to(kSymBand ? j - 2 : (two ? j : j - 1));
+        } else {
             __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[kRvMax + bs0]);  // rows v0-2, v0-1: unused by ref25
-        }
-        rj = rj + 1 == 6 ? 0 : rj + 1;
-        oj = (oj + 1) & 3;
-    }
-    // band rows of the last two steps are never the v-2 row of a later step
-    if (kSymBand && nsteps >= 4) {
-        __syncwarp();
-        if (lane == 0) {
-            mbar_arrive(&empty[kRvMax + bs0]);
-            mbar_arrive(&empty[kRvMax + ring_prev(bs0, Rb)]);
+            if (!kSymBand) release_bands_to(bwait);  // rows v0-2, v0-1: unused by ref25
         }
     }
+    __syncwarp();
+    release_bands_to(nband);
 }
 
 template <class TLo, int OPLO, int OPHI, bool MIXED>

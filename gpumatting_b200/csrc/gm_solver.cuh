@@ -72,7 +72,11 @@ __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize
 
 // Prefetch depths: Krylov sweeps are the hot path; replacement and Jacobi
 // sweeps (rare, FP32 planes) run shallower so three CTAs fit per SM.
-__host__ __device__ constexpr int depth_of(int kind, int oplo) { return kind == KIND_KRYLOV ? (oplo == OP_REF25 ? 3 : 4) : 1; }
+__host__ __device__ constexpr int depth_of(int kind, int oplo) { return kind == KIND_KRYLOV ? 3 : 1; }
+
+// Element type of the operand ring in replacement sweeps: FP64 when the
+// solution is kept in FP64 (mixed), FP32 otherwise.
+__host__ __device__ constexpr int ring_esize(bool mixed) { return mixed ? 8 : 4; }
 
 struct Layout {
     int vring_off, bring_off, pring_off, rring_off, full_off, empty_off, red_off, total;
@@ -95,7 +99,7 @@ __host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int oph
     L.vring_off = 0;
     L.bring_off = a128(vcap);
     L.pring_off = L.bring_off + a128(bcap);
-    L.rring_off = L.pring_off + a128(kConsumers * 6 * kRingCols * 8);
+    L.rring_off = L.pring_off + a128(kConsumers * 8 * kRingCols * ring_esize(mixed));
     L.full_off = L.rring_off + a128(kConsumers * 4 * kWarpCols * 4);
     L.empty_off = L.full_off + a128((kRvMax + kRbMax) * 8);
     L.red_off = L.empty_off + a128((kRvMax + kRbMax) * 8);

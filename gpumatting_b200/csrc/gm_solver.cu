@@ -278,43 +278,49 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
         const CUtensorMap* xm = KIND == KIND_KRYLOV ? &A.m_xlo : &A.m_xhi;
         const uint32_t vbytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2] + K.vbytes[3];
         fence_proxy_async();
-        int vs = 0, bs = 0;
-        for (int t = 0; t < nsteps; ++t) {
-            if (*s_abort) break;
-            const int row = v0 - 2 + t;
-            {
-                const uint32_t bit = 1u << vs;
-                if (pp.used_v & bit) {
-                    if (!mbar_wait_bounded(&empty[vs], (pp.empty_v & bit) ? 1u : 0u, A.gb, A.tma_limit_ns)) {
-                        *s_abort = 1;
-                        break;
-                    }
-                    pp.empty_v ^= bit;
-                }
-                pp.used_v |= bit;
-                unsigned char* dst = vring + vs * K.vslot;
-                mbar_arrive_expect_tx(&full[vs], vbytes);
+        // Issue in the consumers' order: super-step j takes vector rows j and
+        // j+1, then band rows up to (its last step) - 2.  Matching the order
+        // keeps the rings deadlock-free for any depth >= 1.
+        int vs = 0, bs = 0, bnext = 0;
+        auto issue_vec = [&](int t) -> bool {
+            const uint32_t bit = 1u << vs;
+            if (pp.used_v & bit) {
+                if (!mbar_wait_bounded(&empty[vs], (pp.empty_v & bit) ? 1u : 0u, A.gb, A.tma_limit_ns)) return false;
+                pp.empty_v ^= bit;
+            }
+            pp.used_v |= bit;
+            unsigned char* dst = vring + vs * K.vslot;
+            mbar_arrive_expect_tx(&full[vs], vbytes);
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (K.vbytes[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, row, &full[vs]);
-                vs = ring_next(vs, K.Rv);
+            for (int i = 0; i < 4; ++i)
+                if (K.vbytes[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, v0 - 2 + t, &full[vs]);
+            vs = ring_next(vs, K.Rv);
+            return true;
+        };
+        auto issue_band = [&](int m) -> bool {
+            const uint32_t bit = 1u << bs;
+            if (pp.used_b & bit) {
+                if (!mbar_wait_bounded(&empty[kRvMax + bs], (pp.empty_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
+                    return false;
+                pp.empty_b ^= bit;
             }
-            if (t < nband) {
-                const uint32_t bit = 1u << bs;
-                if (pp.used_b & bit) {
-                    if (!mbar_wait_bounded(&empty[kRvMax + bs], (pp.empty_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns)) {
-                        *s_abort = 1;
-                        break;
-                    }
-                    pp.empty_b ^= bit;
-                }
-                pp.used_b |= bit;
-                unsigned char* dst = bring + bs * K.bslot;
-                mbar_arrive_expect_tx(&full[kRvMax + bs], K.bbytes);
-                tma_load_3d(dst, bm, u0 - 8, row, 0, &full[kRvMax + bs]);
-                if (K.xoff >= 0) tma_load_2d(dst + K.xoff, xm, u0 - 8, row, &full[kRvMax + bs]);
-                bs = ring_next(bs, K.Rb);
-            }
+            pp.used_b |= bit;
+            unsigned char* dst = bring + bs * K.bslot;
+            mbar_arrive_expect_tx(&full[kRvMax + bs], K.bbytes);
+            tma_load_3d(dst, bm, u0 - 8, v0 - 2 + m, 0, &full[kRvMax + bs]);
+            if (K.xoff >= 0) tma_load_2d(dst + K.xoff, xm, u0 - 8, v0 - 2 + m, &full[kRvMax + bs]);
+            bs = ring_next(bs, K.Rb);
+            return true;
+        };
+        for (int j = 0; j < nsteps; j += 2) {
+            if (*s_abort) break;
+            const bool two = j + 1 < nsteps;
+            if (!issue_vec(j) || (two && !issue_vec(j + 1))) { *s_abort = 1; break; }
+            const int mneed = (two ? j + 1 : j) - 2;
+            bool ok = true;
+            for (; bnext <= mneed && bnext < nband; ++bnext)
+                if (!issue_band(bnext)) { ok = false; break; }
+            if (!ok) { *s_abort = 1; break; }
         }
         return;
     }

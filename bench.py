@@ -289,9 +289,9 @@ def run_ours(args):
     alpha = torch.empty((H, W), dtype=torch.float32, device=dev)
     store = api.LevinStore(W, H, args.precision)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MB > L2
-    params = dict(rtol=1e-6, max_iters=5000, replace_every=args.replace_every)
+    params = dict(rtol=1e-6, max_iters=5000, replace_every=args.replace_every, ctas_per_sm=args.ctas_per_sm)
     if args.fixed_iters:
-        params = dict(rtol=0.0, max_iters=args.fixed_iters, replace_every=args.replace_every)
+        params.update(rtol=0.0, max_iters=args.fixed_iters)
 
     def step_device():
         store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
@@ -445,6 +445,7 @@ def main():
     ap.add_argument("--fixed-iters", type=int, default=0, help="profiling: run exactly this many CG iterations")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--replace-every", type=int, default=50)
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="ring configuration: 0 auto, 3 shallow, 2 deep")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -246,11 +246,11 @@ __device__ __forceinline__ void load_rows(V (&X)[6][6], const V* ring, int r0, i
     }
 }
 
-template <class TLo, int OPLO, int OPHI, bool MIXED, int KIND>
+template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, int KIND>
 __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* smem, int u0, int v0, int v1,
                                           const KState& s, double (&part)[kNPart], Pipe& pp)
 {
-    constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED);
+    constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED, CFG);
     constexpr KindLayout K = L.k[KIND];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nsteps = v1 - v0 + 4;
@@ -624,12 +624,12 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     release_bands_to(nband);
 }
 
-template <class TLo, int OPLO, int OPHI, bool MIXED>
+template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG>
 __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant__ SolverArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;
-    constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED);
+    constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED, CFG);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     double* red = reinterpret_cast<double*>(smem + L.red_off);
@@ -695,11 +695,11 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
         double part[kNPart] = {0.0, 0.0, 0.0, 0.0};
         if (active) {
             if (kind == KIND_KRYLOV)
-                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_KRYLOV>(A, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, smem, u0, v0, v1, s, part, pp);
             else if (kind == KIND_REPLACE)
-                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_REPLACE>(A, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_REPLACE>(A, smem, u0, v0, v1, s, part, pp);
             else
-                run_sweep<TLo, OPLO, OPHI, MIXED, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, pp);
         }
         block_sum<kNPart>(part, red);
         double* slot = A.partials + (size_t)parity * G * kNPart + blockIdx.x;

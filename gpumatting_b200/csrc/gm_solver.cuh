@@ -42,7 +42,7 @@ __host__ __device__ constexpr int a128(int x) { return (x + 127) & ~127; }
 
 // Vector rows per step: Krylov r, q, p, x increment; replacement base (FP64,
 // mixed only), x increment, p, b; Jacobi x, -, -, b.
-__host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize, bool mixed, int D)
+__host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize, bool mixed, int Rv, int Rb)
 {
     KindLayout K{};
     const int vb4 = kBox * 4;
@@ -64,15 +64,26 @@ __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize
     K.xoff = sym ? a128(pbytes) : -1;
     K.bbytes = pbytes + (sym ? kBox * 4 : 0);
     K.bslot = sym ? a128(K.xoff + kBox * 4) : a128(pbytes);
-    K.D = D;
-    K.Rv = D + 1;
-    K.Rb = D + (sym ? 3 : 1);
+    K.D = Rv - 1;
+    K.Rv = Rv;
+    K.Rb = Rb;
     return K;
 }
 
-// Prefetch depths: Krylov sweeps are the hot path; replacement and Jacobi
-// sweeps (rare, FP32 planes) run shallower so three CTAs fit per SM.
-__host__ __device__ constexpr int depth_of(int kind, int oplo) { return kind == KIND_KRYLOV ? 3 : 1; }
+// Ring slots per kind for a depth configuration.  A super-step holds two
+// vector slots and (symmetric store) four band slots, so Rv >= 2 and
+// Rb >= 4 (2 for the reference layout) always make progress; extra slots
+// are prefetch.  Config 0 fits three CTAs per SM (mixed FP16/BF16), config 1
+// trades one CTA per SM for rings about twice as deep.
+__host__ __device__ constexpr int rings_v(int kind, int oplo, int cfg)
+{
+    return kind == KIND_KRYLOV ? (cfg == 1 && oplo == OP_SYMD ? 8 : 4) : (cfg == 1 && oplo == OP_SYMD ? 3 : 2);
+}
+__host__ __device__ constexpr int rings_b(int kind, int oplo, int cfg)
+{
+    return kind == KIND_KRYLOV ? (oplo == OP_REF25 ? 4 : (cfg == 1 ? 10 : 7))
+                               : (oplo == OP_REF25 ? 2 : (cfg == 1 ? 6 : 4));
+}
 
 // Element type of the operand ring in replacement sweeps: FP64 when the
 // solution is kept in FP64 (mixed), FP32 otherwise.
@@ -85,12 +96,12 @@ struct Layout {
 
 __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 
-__host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int ophi, bool mixed)
+__host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int ophi, bool mixed, int cfg)
 {
     Layout L{};
-    L.k[KIND_KRYLOV] = kind_layout(KIND_KRYLOV, oplo, esize_lo, mixed, depth_of(KIND_KRYLOV, oplo));
-    L.k[KIND_REPLACE] = kind_layout(KIND_REPLACE, ophi, 4, mixed, depth_of(KIND_REPLACE, oplo));
-    L.k[KIND_JACOBI] = kind_layout(KIND_JACOBI, ophi, 4, mixed, depth_of(KIND_JACOBI, oplo));
+    for (int k = 0; k < NKIND; ++k)
+        L.k[k] = kind_layout(k, k == KIND_KRYLOV ? oplo : ophi, k == KIND_KRYLOV ? esize_lo : 4, mixed,
+                             rings_v(k, oplo, cfg), rings_b(k, oplo, cfg));
     int vcap = 0, bcap = 0;
     for (int k = 0; k < NKIND; ++k) {
         vcap = imax(vcap, L.k[k].Rv * L.k[k].vslot);

@@ -292,114 +292,6 @@ __device__ __forceinline__ void grid_total(const double* p, int n, double (&out)
     __syncthreads();
 }
 
-// Hierarchical barrier + deterministic reduction state (zeroed before the
-// launch).  CTAs are split into at most 32 groups of consecutive CTAs; each
-// group has its own counter line, so arrivals do not pile onto one address.
-struct GroupState {
-    unsigned count;
-    unsigned pad[31];
-};
-constexpr int kMaxGroups = 32;
-
-// Reduction of NV per-CTA partials across the grid, fused with the grid
-// barrier.  Every CTA writes its block totals (valid in thread 0) to
-// part[k * G + cta]; the last arriver of each group sums its members in
-// CTA order into gtot[g]; the last group sums gtot[] in group order into
-// tot[] and releases the barrier.  The sums therefore use the same order
-// whatever the arrival order, and every CTA reads the same totals.  Returns
-// false when the barrier was abandoned (limit or abort).  extra > 0 makes
-// group 0 wait for arrivals that never come (test hook).
-template <int NV>
-__device__ __forceinline__ bool grid_reduce(GridBarrier* gb, GroupState* groups, double* part, double* gtot,
-                                            double* tot, unsigned G, unsigned extra, uint64_t limit_ns,
-                                            const double (&mine)[NV], double (&out)[NV], double* smem_bcast)
-{
-    __shared__ int s_ok;
-    const unsigned GS = (G + kMaxGroups - 1) / kMaxGroups;
-    const unsigned NG = (G + GS - 1) / GS;
-    const unsigned cta = blockIdx.x, g = cta / GS;
-    const unsigned g0 = g * GS, gsize = min(GS, G - g0) + (g == 0 ? extra : 0u);
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        int ok = 1;
-        unsigned gen0 = 0, last_g = 0;
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) part[(size_t)k * G + cta] = mine[k];
-            gen0 = ld_acquire(&gb->gen);
-            __threadfence();
-            last_g = atomicAdd(&groups[g].count, 1u) == gsize - 1 ? 1u : 0u;
-        }
-        last_g = __shfl_sync(0xffffffffu, last_g, 0);
-        gen0 = __shfl_sync(0xffffffffu, gen0, 0);
-        bool released = false;
-        if (last_g) {
-            __threadfence();
-            double v[NV];
-#pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                double x = 0.0;
-                for (unsigned m = lane; m < gsize && g0 + m < G; m += 32) x += __ldcg(part + (size_t)k * G + g0 + m);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-                v[k] = x;
-            }
-            unsigned last_t = 0;
-            if (lane == 0) {
-#pragma unroll
-                for (int k = 0; k < NV; ++k) gtot[g * NV + k] = v[k];
-                groups[g].count = 0;
-                __threadfence();
-                last_t = atomicAdd(&groups[kMaxGroups].count, 1u) == NG - 1 ? 1u : 0u;
-            }
-            last_t = __shfl_sync(0xffffffffu, last_t, 0);
-            if (last_t) {
-                __threadfence();
-#pragma unroll
-                for (int k = 0; k < NV; ++k) {
-                    double x = (unsigned)lane < NG ? __ldcg(gtot + lane * NV + k) : 0.0;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-                    if (lane == 0) tot[k] = x;
-                }
-                if (lane == 0) {
-                    groups[kMaxGroups].count = 0;
-                    __threadfence();
-                    st_release(&gb->gen, gen0 + 1);
-                }
-                released = true;
-            }
-        }
-        if (lane == 0 && !released) {
-            const uint64_t t0 = globaltimer_ns();
-            unsigned spins = 0;
-            while (ld_acquire(&gb->gen) == gen0) {
-                if (ld_volatile_int(&gb->abort)) { ok = 0; break; }
-                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) {
-                    atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
-                    atomicExch(&gb->where, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        if (lane == 0) {
-            __threadfence();
-            if (ld_volatile_int(&gb->abort)) ok = 0;
-            s_ok = ok;
-        }
-        __syncwarp();
-        if (lane < NV) smem_bcast[lane] = __ldcg(tot + lane);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = smem_bcast[k];
-    const bool ok = s_ok != 0;
-    __syncthreads();
-    return ok;
-}
-
 template <class T> struct Cvt;
 template <> struct Cvt<float> {
     static __device__ __forceinline__ float to_f(float x) { return x; }

@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     const unsigned G = gridDim.x;
     bool ok = grid_sync(A.gb, G + (A.inject == 1 ? 1u : 0u), A.limit_ns);
 
-    int status = GM_OK, it = 0, nrep = 0;
+    int status = GM_OK, it = 0, nrep = 0, parity = 0;
     int kind = jac ? KIND_JACOBI : KIND_REPLACE;
     KState s;
     s.af = 0.f; s.bf = 0.f; s.ad = 0.0; s.skipR = true; s.beta_zero = true; s.c = 0; s.xsel = 0;
@@ -702,9 +702,16 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, pp);
         }
         block_sum<kNPart>(part, red);
-        double tot[kNPart];
-        ok = grid_reduce<kNPart>(A.gb, A.groups, A.partials, A.gtot, A.tot, G, 0u, A.limit_ns, part, tot, red);
+        double* slot = A.partials + (size_t)parity * G * kNPart + blockIdx.x;
+        if (tid == 0) {
+#pragma unroll
+            for (int k = 0; k < kNPart; ++k) slot[(size_t)k * G] = part[k];
+        }
+        ok = grid_sync(A.gb, G, A.limit_ns);
         if (!ok) break;
+        double tot[kNPart];
+        grid_total<kNPart>(A.partials + (size_t)parity * G * kNPart, (int)G, tot, red);
+        parity ^= 1;
 
         if (kind == KIND_KRYLOV) {
             s.c ^= 1;

@@ -146,10 +146,7 @@ struct SolverArgs {
     int P;                    // pitch (elements) of the work vectors
     int W, H;
     int nstrips, nseg, nunits;
-    double* partials;         // [kNPart][grid] per-CTA sums of the current sweep
-    double* gtot;             // [kMaxGroups][kNPart] group sums
-    double* tot;              // [kNPart] grid sums
-    GroupState* groups;       // [kMaxGroups + 1] counters (zeroed before launch)
+    double* partials;         // [2][kNPart][grid]
     GridBarrier* gb;
     SolverOut* out;
     // parameters

@@ -292,6 +292,110 @@ __device__ __forceinline__ void grid_total(const double* p, int n, double (&out)
     __syncthreads();
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Grid barrier fused with a deterministic all-reduce of NV doubles per
+// thread.  On return every thread of every CTA holds the same bit-identical
+// grid totals in v.  parts is [NV][G] global scratch for this call (callers
+// alternate two copies so a fast CTA's next call cannot overwrite partials a
+// slow CTA is still reading).  scratch: >= 32 * NV + NV shared doubles.
+//
+// One warp does the grid part: lane 0 publishes the CTA sum and arrives with
+// an acquire-release atomic (its release covers every write the CTA made
+// before the first __syncthreads), spins on the generation with acquire
+// loads, and the warp then adds the G partials in a fixed order.  Two
+// __syncthreads per call in total.  Returns false when the barrier was
+// abandoned (limit reached or abort set by another CTA).
+template <int NV>
+__device__ __forceinline__ bool grid_allreduce(GridBarrier* gb, double* parts, unsigned G, uint64_t limit_ns,
+                                               double (&v)[NV], double* scratch)
+{
+    __shared__ int s_ok;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) scratch[wid * NV + k] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        double cs[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? scratch[lane * NV + k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            cs[k] = x;
+        }
+        int ok = 1;
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) parts[(size_t)k * G + blockIdx.x] = cs[k];
+            const unsigned g = ld_acquire(&gb->gen);
+            const unsigned arrived = atom_add_acq_rel(&gb->count, 1u);
+            if (arrived == G - 1) {
+                gb->count = 0;
+                st_release(&gb->gen, g + 1);
+            } else {
+                uint64_t t0 = 0;
+                unsigned spins = 0;
+                while (ld_acquire(&gb->gen) == g) {
+                    ++spins;
+                    if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) { ok = 0; break; }
+                    if ((spins & 63u) == 0) {
+                        const uint64_t now = globaltimer_ns();
+                        if (t0 == 0) t0 = now;
+                        else if (now - t0 > limit_ns) {
+                            atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
+                            atomicExch(&gb->where, 1);
+                            ok = 0;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) {
+            double a[NV], b[NV];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) { a[k] = 0.0; b[k] = 0.0; }
+            int i = lane;
+            for (; i + 32 < (int)G; i += 64) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    a[k] += __ldcg(parts + (size_t)k * G + i);
+                    b[k] += __ldcg(parts + (size_t)k * G + i + 32);
+                }
+            }
+            if (i < (int)G) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) a[k] += __ldcg(parts + (size_t)k * G + i);
+            }
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                double x = a[k] + b[k];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+                if (lane == 0) scratch[32 * NV + k] = x;
+            }
+        }
+        if (lane == 0) s_ok = ok;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = scratch[32 * NV + k];
+    return s_ok != 0;
+}
+
 template <class T> struct Cvt;
 template <> struct Cvt<float> {
     static __device__ __forceinline__ float to_f(float x) { return x; }

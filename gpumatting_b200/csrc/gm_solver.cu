@@ -259,7 +259,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     unsigned char* vring = smem + L.vring_off;
     unsigned char* bring = smem + L.bring_off;
-    volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + 32 * kNPart * 8);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + kRedBytes);
     constexpr bool kSymBand = (KIND == KIND_KRYLOV ? OPLO : OPHI) != OP_REF25;
 
     if (warp == kConsumers) {
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], kConsumers);
         }
-        *reinterpret_cast<volatile int*>(smem + L.red_off + 32 * kNPart * 8) = 0;
+        *reinterpret_cast<volatile int*>(smem + L.red_off + kRedBytes) = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -701,16 +701,9 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
             else
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, pp);
         }
-        block_sum<kNPart>(part, red);
-        double* slot = A.partials + (size_t)parity * G * kNPart + blockIdx.x;
-        if (tid == 0) {
-#pragma unroll
-            for (int k = 0; k < kNPart; ++k) slot[(size_t)k * G] = part[k];
-        }
-        ok = grid_sync(A.gb, G, A.limit_ns);
+        ok = grid_allreduce<kNPart>(A.gb, A.partials + (size_t)parity * G * kNPart, G, A.limit_ns, part, red);
         if (!ok) break;
-        double tot[kNPart];
-        grid_total<kNPart>(A.partials + (size_t)parity * G * kNPart, (int)G, tot, red);
+        const double (&tot)[kNPart] = part;
         parity ^= 1;
 
         if (kind == KIND_KRYLOV) {

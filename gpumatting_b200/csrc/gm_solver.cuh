@@ -21,6 +21,7 @@ constexpr int kRingCols = kWarpCols + 4;         // private operand ring: warp c
 constexpr int kRvMax = 16;                       // vector ring slots
 constexpr int kRbMax = 16;                       // band ring slots
 constexpr int kNPart = 4;                        // FP64 partial sums per CTA per sweep
+constexpr int kRedBytes = (32 + 1) * kNPart * 8;  // reduction scratch: warp sums + grid totals
 
 // Shared-memory carve of one sweep kind.  Everything here is a compile-time
 // function of the operator types, so the hot loop indexes rings with
@@ -114,7 +115,7 @@ __host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int oph
     L.full_off = L.rring_off + a128(kConsumers * 4 * kWarpCols * 4);
     L.empty_off = L.full_off + a128((kRvMax + kRbMax) * 8);
     L.red_off = L.empty_off + a128((kRvMax + kRbMax) * 8);
-    L.total = L.red_off + a128(32 * kNPart * 8 + 16);
+    L.total = L.red_off + a128(kRedBytes + 16);  // + abort flag
     return L;
 }
 

@@ -87,6 +87,7 @@ SIGNATURES = {
     "gm_jacobi_step": (_i, [_vp, _vp, BandedMatrix, _vp, _f, _vp]),
     "gm_inner_prod": (_i, [_vp, _vp, _vp, _i, _vp]),
     "gm_inner_prod_f64": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "gm_inner_prod_f64_noalloc": (_i, [_vp, _vp, _vp, _i, _vp]),
     "gm_vec_add": (_i, [_vp, _vp, _vp, _i, _vp]),
     "gm_vec_sub": (_i, [_vp, _vp, _vp, _i, _vp]),
     "gm_vec_scale_const": (_i, [_vp, _vp, _f, _i, _vp]),

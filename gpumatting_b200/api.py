@@ -179,6 +179,13 @@ def inner_prod(x, y, stream=None, f64: bool = False):
     return out
 
 
+def inner_prod_noalloc(x, y, out, stream=None):
+    """<x, y> in FP64 into the device double `out`, allocating nothing."""
+    L.check(L.load().gm_inner_prod_f64_noalloc(out.data_ptr(), x.data_ptr(), y.data_ptr(), x.numel(),
+                                               _stream(stream)))
+    return out
+
+
 def compute_error(alpha, gt, W: int, H: int, stream=None) -> float:
     v = C.c_double(0)
     L.check(L.load().gm_compute_error(C.byref(v), alpha.data_ptr(), gt.data_ptr(), W, H, _stream(stream)))

@@ -203,3 +203,61 @@ extern "C" void computeError(float* alpha, float* gtAlpha, int imW, int imH)
     gm_note_status(rc);
     if (rc == GM_OK) printf("Ground truth MSE: %.3e\n", mse);
 }
+
+// ---- allocation-free dot product ----
+//
+// For callers that may not allocate device memory while they run: code that
+// hands all device memory to its own allocator or runs under a fixed memory
+// budget, and latency-critical loops where a stream-ordered allocation that
+// grows the pool would stall.  The partial sums live in a fixed file-scope
+// device array instead of a cudaMallocAsync buffer.  Every block writes its
+// own slot before the finishing pass reads it, so nothing has to start at
+// zero.  Calls that overlap in time on one device (different streams or
+// host threads) share the array and race; serialise them.
+namespace gm {
+constexpr int kStaticDotParts = 4096;  // 32 KB of partials per device
+__device__ __align__(256) double g_static_dot_parts[kStaticDotParts];
+}  // namespace gm
+
+#include <mutex>
+
+static double* static_dot_parts(int dev)
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static double* addr[kMaxDevices] = {};
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        // The current device is dev, so the symbol resolves in its context.
+        if (cudaGetSymbolAddress(&p, gm::g_static_dot_parts) != cudaSuccess) return nullptr;
+        addr[dev] = static_cast<double*>(p);
+    }
+    return addr[dev];
+}
+
+extern "C" int gm_inner_prod_f64_noalloc(double* result, const float* x, const float* y, int len, void* stream)
+{
+    if (len < 0 || !result) { gm_set_error_msg("bad inner product arguments"); return GM_ERR_INVALID; }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (len == 0) {
+        GM_CUDA_TRY(cudaMemsetAsync(result, 0, sizeof(double), st));
+        return GM_OK;
+    }
+    if (!x || !y) { gm_set_error_msg("NULL vector"); return GM_ERR_INVALID; }
+    int dev = 0;
+    GM_CUDA_TRY(cudaGetDevice(&dev));
+    const int nb = dot_blocks(len);
+    if (nb > kStaticDotParts) {
+        gm_set_error_msg("inner product needs %d partial sums; the static scratch holds %d", nb, kStaticDotParts);
+        return GM_ERR_INVALID;
+    }
+    double* parts = static_dot_parts(dev);
+    if (!parts) {
+        cudaGetLastError();
+        gm_set_error_msg("cannot resolve the static dot-product scratch on device %d", dev);
+        return GM_ERR_CUDA;
+    }
+    return dot_with_scratch(x, y, len, parts, nb, nullptr, result, st);
+}

@@ -127,6 +127,18 @@ int gm_jacobi_step(float* xx, const float* x, BandedMatrix a, const float* b, fl
 int gm_inner_prod(float* result, const float* x, const float* y, int len, void* stream);
 /* FP64 result, written to a device double. */
 int gm_inner_prod_f64(double* result, const float* x, const float* y, int len, void* stream);
+/* Same result as gm_inner_prod_f64, bit for bit, with no device allocation:
+ * the per-block partial sums go to a fixed 4096-double array inside the
+ * library (one per device) instead of a stream-ordered buffer.  For callers
+ * that must not allocate while they run (their own allocator owns device
+ * memory, or a latency-critical loop cannot afford pool growth).  No
+ * counterpart in the reference, whose innerProd allocates nothing but races
+ * between blocks (Vector.cu:195-265).  Limits: lengths whose launch would need
+ * more than 4096 partials are rejected (GM_ERR_INVALID; never on a 148-SM
+ * B200, which uses at most 592); calls that overlap in time on one device
+ * share the array and race, so serialise them; make the first call on each
+ * device outside stream capture, since it resolves the array's address. */
+int gm_inner_prod_f64_noalloc(double* result, const float* x, const float* y, int len, void* stream);
 /* Vector.cu:124-183 */
 int gm_vec_add(float* result, const float* x, const float* y, int len, void* stream);
 int gm_vec_sub(float* result, const float* x, const float* y, int len, void* stream);

@@ -256,6 +256,8 @@ class LevinStore:
         bm = None if bands25 is None else C.byref(bands25.struct)
         L.check(L.load().gm_levin_assemble(C.byref(self.s), C.byref(im), C.byref(sc), eps, bm, _ptr(b25),
                                            _stream(stream)))
+        # The adjoint recomputes window statistics from the same inputs.
+        self._inputs = (image, scribbles, eps, gamma_value, gamma_map, s_map)
         return self
 
     def planes(self, which: str = "w32"):
@@ -285,6 +287,43 @@ class LevinStore:
         if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
             L.check(rc)
         return SolveResult.from_info(info)
+
+
+    def solve_rhs(self, rhs, x, solver: str = "cg", stream=None, **params) -> SolveResult:
+        """Solve the store's system for rhs ([H, W] device floats); x holds the
+        initial guess and receives the solution."""
+        p = L.default_params(solver=SOLVERS[solver], **params)
+        info = L.GmSolveInfo()
+        rc = L.load().gm_levin_solve_rhs(C.byref(self.s), rhs.data_ptr(), x.data_ptr(), C.byref(p), C.byref(info),
+                                         _stream(stream))
+        if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
+            L.check(rc)
+        return SolveResult.from_info(info)
+
+    def adjoint(self, alpha, dalpha, solver: str = "cg", want_dgamma: bool = True, stream=None, **params):
+        """Gradients of a loss of alpha through solve and assembly.
+
+        dalpha = dloss/dalpha ([H, W] device floats).  Returns (dimage, dgamma,
+        lam, SolveResult of the lam solve): dimage has the channel count of the
+        assembled image layout (3 for RGB8, 4 for RGBA32F with the last 0) and
+        is the gradient for the [0, 1] channel values."""
+        torch = _torch()
+        image, scribbles, eps, gamma_value, gamma_map, s_map = self._inputs
+        W, H = self.W, self.H
+        ch = 4 if image.dtype == torch.float32 else 3
+        dimage = torch.empty((H, W, ch), dtype=torch.float32, device=alpha.device)
+        lam = torch.empty((H, W), dtype=torch.float32, device=alpha.device)
+        dgamma = torch.empty((H, W), dtype=torch.float32, device=alpha.device) if want_dgamma else None
+        im = _image_desc(image)
+        sc = _scrib_desc(scribbles, gamma_value, gamma_map, s_map)
+        p = L.default_params(solver=SOLVERS[solver], **params)
+        info = L.GmSolveInfo()
+        rc = L.load().gm_levin_adjoint(C.byref(self.s), C.byref(im), C.byref(sc), eps, alpha.data_ptr(),
+                                       dalpha.data_ptr(), lam.data_ptr(), dimage.data_ptr(), W * ch, ch,
+                                       _ptr(dgamma), C.byref(p), C.byref(info), _stream(stream))
+        if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
+            L.check(rc)
+        return dimage, dgamma, lam, SolveResult.from_info(info)
 
 
 class _CudaArray:

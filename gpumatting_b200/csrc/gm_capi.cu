@@ -120,12 +120,13 @@ extern "C" int gm_banded_solve(BandedMatrix L, int W, float* alpha, int pad, con
     return rc;
 }
 
-extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const gm_solve_params* prm,
-                              gm_solve_info* info, void* stream)
+// Solves the store's system for right-hand side b ([H][bpitch] floats).
+static int levin_solve_impl(const gm_levin_store* store, const float* b, int bpitch, float* alpha,
+                            const gm_solve_params* prm, gm_solve_info* info, void* stream)
 {
     gm_solve_params p;
     if (prm) p = *prm; else gm_default_params(&p);
-    if (!store || !store->w32 || !alpha) { gm_set_error_msg("gm_levin_solve: bad arguments"); return GM_ERR_INVALID; }
+    if (!store || !store->w32 || !alpha || !b) { gm_set_error_msg("gm_levin_solve: bad arguments"); return GM_ERR_INVALID; }
     const int W = store->W, H = store->H, P = store->pitch;
     SolverSetup S;
     memset(&S, 0, sizeof(S));
@@ -156,12 +157,49 @@ extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const g
     S.xlo_pitch = P;
     S.xhi = store->gamma;
     S.xhi_pitch = P;
-    S.b = store->b;
-    S.bpitch = P;
+    S.b = b;
+    S.bpitch = bpitch;
     S.alpha_in = alpha;
     S.alpha_out = alpha;
     S.alpha_pitch = W;
     return run_solver(S, &p, info, (cudaStream_t)stream);
+}
+
+extern "C" int gm_levin_solve(const gm_levin_store* store, float* alpha, const gm_solve_params* prm,
+                              gm_solve_info* info, void* stream)
+{
+    if (!store) { gm_set_error_msg("gm_levin_solve: bad arguments"); return GM_ERR_INVALID; }
+    return levin_solve_impl(store, store->b, store->pitch, alpha, prm, info, stream);
+}
+
+extern "C" int gm_levin_solve_rhs(const gm_levin_store* store, const float* rhs, float* x,
+                                  const gm_solve_params* prm, gm_solve_info* info, void* stream)
+{
+    if (!store) { gm_set_error_msg("gm_levin_solve_rhs: bad arguments"); return GM_ERR_INVALID; }
+    return levin_solve_impl(store, rhs, store->W, x, prm, info, stream);
+}
+
+int gm_levin_adjoint_grads(const gm_image* im, const gm_scribbles* sc, double eps, int W, int H,
+                           const float* lam, const float* alpha, float* dimage, size_t dimage_pitch,
+                           int dimage_channels, float* dgamma, cudaStream_t stream);
+
+extern "C" int gm_levin_adjoint(const gm_levin_store* store, const gm_image* im, const gm_scribbles* sc,
+                                double eps, const float* alpha, const float* dalpha, float* lambda,
+                                float* dimage, size_t dimage_pitch, int dimage_channels, float* dgamma,
+                                const gm_solve_params* prm, gm_solve_info* info, void* stream)
+{
+    if (!store || !store->w32 || !alpha || !dalpha || !lambda || !dimage) {
+        gm_set_error_msg("gm_levin_adjoint: bad arguments");
+        return GM_ERR_INVALID;
+    }
+    const int W = store->W, H = store->H;
+    cudaStream_t st = (cudaStream_t)stream;
+    GM_CUDA_TRY(cudaMemsetAsync(lambda, 0, sizeof(float) * (size_t)W * H, st));
+    const int rc = levin_solve_impl(store, dalpha, W, lambda, prm, info, stream);
+    if (rc != GM_OK && rc != GM_ERR_NOT_CONVERGED) return rc;
+    GM_TRY(gm_levin_adjoint_grads(im, sc, eps, W, H, lambda, alpha, dimage, dimage_pitch, dimage_channels, dgamma,
+                                  st));
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

@@ -364,6 +364,142 @@ static void launch_sym(const ImgView& im, const ScribView& sc, double eps, int W
     levin_diag_kernel<T><<<g2, 128, 0, st>>>(reinterpret_cast<const T*>(o.w), o.w32, o.gamma, d, d32, W, H, o.pitch);
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint of the assembly
+// ---------------------------------------------------------------------------
+// For a loss of alpha with lam = A^-1 dloss/dalpha (A is symmetric), every
+// pair (i, j) the store couples has dloss/dw_ij = -(lam_i - lam_j)(alpha_i -
+// alpha_j), and each window k adds w_ij += (1 + x_i^T K^-1 x_j) / 9 with
+// x = I - mu_k and K = Sigma_k + eps/9 I.  Summing the pair gradients of one
+// window collapses to two 3-vectors,
+//   ka = K^-1 sum_a x_a alpha_a,   kl = K^-1 sum_a x_a lam_a,
+// and pixel a of the window receives
+//   dI_a += [(lam_a - mean lam) ka + (alpha_a - mean alpha) kl] / 9
+//           - [(x_a . kl) ka + (x_a . ka) kl] / 81.
+// The window statistics are recomputed from the image (the forward pass
+// stores none).  FP64 throughout, one FP32 rounding per output.
+
+// Scribble target s_i: the value b_i / gamma_i the forward pass encodes
+// (0 where the pixel carries no scribble).
+__device__ __forceinline__ float scribble_target(const ScribView& s, int u, int v)
+{
+    if (s.gamma_map) return s.s_map ? s.s_map[(size_t)v * s.W + u] : 0.f;
+    if (s.map) return s.map[(size_t)v * s.map_pitch + u] == 255 ? 1.f : 0.f;
+    return 0.f;
+}
+
+struct AdjOut {
+    float* dimage;   // [H][dpitch] floats, `channels` per pixel
+    size_t dpitch;
+    int channels;    // 3 or 4 (the fourth is written as 0)
+    float* dgamma;   // [H][W] or NULL
+};
+
+__global__ void __launch_bounds__(TW * TH) levin_adjoint_kernel(ImgView im, ScribView sc, double eps, int W, int H,
+                                                                const float* __restrict__ lam,
+                                                                const float* __restrict__ alpha, AdjOut o)
+{
+    __shared__ double col[TH + 4][TW + 4][3];
+    __shared__ double sl[TH + 4][TW + 4];
+    __shared__ double sa[TH + 4][TW + 4];
+    __shared__ double wmu[NWIN][3];
+    __shared__ double wka[NWIN][3];
+    __shared__ double wkl[NWIN][3];
+    __shared__ double wbar[NWIN][2];  // mean lam, mean alpha
+    const int u0 = blockIdx.x * TW, v0 = blockIdx.y * TH;
+    const int tid = threadIdx.x;
+    for (int t = tid; t < (TH + 4) * (TW + 4); t += blockDim.x) {
+        const int x = t % (TW + 4), y = t / (TW + 4);
+        const int u = u0 - 2 + x, v = v0 - 2 + y;
+        double r = 0, g = 0, b = 0, l = 0, a = 0;
+        if (u >= 0 && u < W && v >= 0 && v < H) {
+            load_rgb_d(im, u, v, r, g, b);
+            l = lam[(size_t)v * W + u];
+            a = alpha[(size_t)v * W + u];
+        }
+        col[y][x][0] = r; col[y][x][1] = g; col[y][x][2] = b;
+        sl[y][x] = l;
+        sa[y][x] = a;
+    }
+    __syncthreads();
+    for (int t = tid; t < NWIN; t += blockDim.x) {
+        const int wx = t % (TW + 2), wy = t / (TW + 2);
+        const int cu = u0 - 1 + wx, cv = v0 - 1 + wy;
+        if (cu < 1 || cu > W - 2 || cv < 1 || cv > H - 2) continue;
+        double m[3] = {0, 0, 0}, c[6] = {0, 0, 0, 0, 0, 0}, lb = 0, ab = 0;
+        for (int q = 0; q < 9; ++q) {
+            const double* p = col[wy + q / 3][wx + q % 3];
+            m[0] += p[0]; m[1] += p[1]; m[2] += p[2];
+            c[0] += p[0] * p[0]; c[1] += p[0] * p[1]; c[2] += p[0] * p[2];
+            c[3] += p[1] * p[1]; c[4] += p[1] * p[2]; c[5] += p[2] * p[2];
+            lb += sl[wy + q / 3][wx + q % 3];
+            ab += sa[wy + q / 3][wx + q % 3];
+        }
+        for (int a = 0; a < 3; ++a) m[a] /= 9.0;
+        const double e9 = eps / 9.0;
+        const double s00 = c[0] / 9.0 - m[0] * m[0] + e9, s01 = c[1] / 9.0 - m[0] * m[1],
+                     s02 = c[2] / 9.0 - m[0] * m[2], s11 = c[3] / 9.0 - m[1] * m[1] + e9,
+                     s12 = c[4] / 9.0 - m[1] * m[2], s22 = c[5] / 9.0 - m[2] * m[2] + e9;
+        const double a00 = s11 * s22 - s12 * s12, a01 = s02 * s12 - s01 * s22, a02 = s01 * s12 - s02 * s11;
+        const double a11 = s00 * s22 - s02 * s02, a12 = s02 * s01 - s00 * s12, a22 = s00 * s11 - s01 * s01;
+        const double id = 1.0 / (s00 * a00 + s01 * a01 + s02 * a02);
+        double va[3] = {0, 0, 0}, vl[3] = {0, 0, 0};
+        for (int q = 0; q < 9; ++q) {
+            const double* p = col[wy + q / 3][wx + q % 3];
+            const double l = sl[wy + q / 3][wx + q % 3], a = sa[wy + q / 3][wx + q % 3];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const double x = p[e] - m[e];
+                va[e] += x * a;
+                vl[e] += x * l;
+            }
+        }
+        wmu[t][0] = m[0]; wmu[t][1] = m[1]; wmu[t][2] = m[2];
+        wka[t][0] = (a00 * va[0] + a01 * va[1] + a02 * va[2]) * id;
+        wka[t][1] = (a01 * va[0] + a11 * va[1] + a12 * va[2]) * id;
+        wka[t][2] = (a02 * va[0] + a12 * va[1] + a22 * va[2]) * id;
+        wkl[t][0] = (a00 * vl[0] + a01 * vl[1] + a02 * vl[2]) * id;
+        wkl[t][1] = (a01 * vl[0] + a11 * vl[1] + a12 * vl[2]) * id;
+        wkl[t][2] = (a02 * vl[0] + a12 * vl[1] + a22 * vl[2]) * id;
+        wbar[t][0] = lb / 9.0;
+        wbar[t][1] = ab / 9.0;
+    }
+    __syncthreads();
+    const int lx = tid % TW, ly = tid / TW;
+    const int u = u0 + lx, v = v0 + ly;
+    if (u >= W || v >= H) return;
+    const double* xi = col[ly + 2][lx + 2];
+    const double li = sl[ly + 2][lx + 2], ai = sa[ly + 2][lx + 2];
+    double g[3] = {0, 0, 0};
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int cu = u + dx, cv = v + dy;
+            if (cu < 1 || cu > W - 2 || cv < 1 || cv > H - 2) continue;
+            const int t = (ly + 1 + dy) * (TW + 2) + (lx + 1 + dx);
+            const double x0 = xi[0] - wmu[t][0], x1 = xi[1] - wmu[t][1], x2 = xi[2] - wmu[t][2];
+            const double* ka = wka[t];
+            const double* kl = wkl[t];
+            const double xkl = x0 * kl[0] + x1 * kl[1] + x2 * kl[2];
+            const double xka = x0 * ka[0] + x1 * ka[1] + x2 * ka[2];
+            const double dl = (li - wbar[t][0]) / 9.0 - xkl / 81.0;
+            const double da = (ai - wbar[t][1]) / 9.0 - xka / 81.0;
+#pragma unroll
+            for (int e = 0; e < 3; ++e) g[e] += dl * ka[e] + da * kl[e];
+        }
+    }
+    float* out = o.dimage + (size_t)v * o.dpitch + (size_t)o.channels * u;
+    out[0] = __double2float_rn(g[0]);
+    out[1] = __double2float_rn(g[1]);
+    out[2] = __double2float_rn(g[2]);
+    if (o.channels == 4) out[3] = 0.f;
+    if (o.dgamma) {
+        const double s = scribble_target(sc, u, v);
+        o.dgamma[(size_t)v * W + u] = __double2float_rn(li * (s - ai));
+    }
+}
+
 }  // namespace gm
 
 using namespace gm;
@@ -489,6 +625,30 @@ extern "C" int gm_levin_assemble_bands25(float* a, size_t apitch, float* b, cons
         gm_levin_store_free(&tmp);
         if (rc != GM_OK) return rc;
     }
+    GM_CUDA_TRY(cudaGetLastError());
+    return GM_OK;
+}
+
+// Image and scribble-weight gradients from lam and alpha (both [H][W] floats
+// on the device).  Used by gm_levin_adjoint after its lam solve.
+int gm_levin_adjoint_grads(const gm_image* im, const gm_scribbles* sc, double eps, int W, int H,
+                           const float* lam, const float* alpha, float* dimage, size_t dimage_pitch,
+                           int dimage_channels, float* dgamma, cudaStream_t stream)
+{
+    if (W <= 0 || H <= 0 || !lam || !alpha || !dimage) { gm_set_error_msg("adjoint: bad arguments"); return GM_ERR_INVALID; }
+    if (dimage_channels != 3 && dimage_channels != 4) { gm_set_error_msg("adjoint: dimage_channels must be 3 or 4"); return GM_ERR_INVALID; }
+    if (dimage_pitch < (size_t)dimage_channels * W) { gm_set_error_msg("adjoint: dimage_pitch below channels * W"); return GM_ERR_INVALID; }
+    if (!(eps >= 0.0)) { gm_set_error_msg("eps must be >= 0"); return GM_ERR_INVALID; }
+    ImgView iv;
+    ScribView sv;
+    GM_TRY(make_views(im, sc, W, iv, sv));
+    AdjOut o;
+    o.dimage = dimage;
+    o.dpitch = dimage_pitch;
+    o.channels = dimage_channels;
+    o.dgamma = dgamma;
+    dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH);
+    levin_adjoint_kernel<<<grid, TW * TH, 0, stream>>>(iv, sv, eps, W, H, lam, alpha, o);
     GM_CUDA_TRY(cudaGetLastError());
     return GM_OK;
 }

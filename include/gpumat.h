@@ -254,6 +254,28 @@ void gm_default_params(gm_solve_params* p);
 int gm_levin_solve(const gm_levin_store* st, float* alpha, const gm_solve_params* p,
                    gm_solve_info* info, void* stream);
 
+/* Solve the store's system for another right-hand side: rhs and x are
+ * device [H][W] floats (pitch W); x holds the initial guess on entry. */
+int gm_levin_solve_rhs(const gm_levin_store* st, const float* rhs, float* x, const gm_solve_params* p,
+                       gm_solve_info* info, void* stream);
+
+/* Adjoint of assemble + solve for a scalar loss of alpha (no counterpart in
+ * the reference, which has no gradients).  Given the solved alpha and
+ * dalpha = dloss/dalpha (device [H][W] floats), solves the symmetric system
+ * (L + diag(gamma)) lambda = dalpha with the store's solver (lambda's input
+ * contents are ignored; it receives lambda), then writes
+ *   dimage: dloss/dI for the [0,1] RGB values the store was assembled from,
+ *           `dimage_channels` (3, or 4 with the fourth set to 0) floats per
+ *           pixel, rows dimage_pitch floats apart;
+ *   dgamma: dloss/dgamma_i = lambda_i (s_i - alpha_i), [H][W], may be NULL
+ *           (s_i is the scribble target, 0 on pixels without one).
+ * im, sc and eps must be the ones the store was assembled with.  Returns the
+ * lambda solve's status (GM_ERR_NOT_CONVERGED still writes the gradients). */
+int gm_levin_adjoint(const gm_levin_store* st, const gm_image* im, const gm_scribbles* sc, double eps,
+                     const float* alpha, const float* dalpha, float* lambda, float* dimage,
+                     size_t dimage_pitch, int dimage_channels, float* dgamma, const gm_solve_params* p,
+                     gm_solve_info* info, void* stream);
+
 /* Solve with a 25-band BandedMatrix on the device (reference layout).
  * W > 0 declares the Levin stencil of an image W wide (rows = W*H) and
  * selects the fused stencil kernel; W = 0 (or offsets that are not the Levin

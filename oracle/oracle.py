@@ -263,3 +263,28 @@ def sym_edge_grad(lam: np.ndarray, alpha: np.ndarray, W: int, H: int) -> np.ndar
         aj = al[dv:dv + v1, u0 + du:u1 + du]
         gw[k - 1, :v1, u0:u1] = -(li - lj) * (ai - aj)
     return gw.reshape(12, W * H)
+
+
+def reference_adjoint(im3: np.ndarray, gamma: np.ndarray, s: np.ndarray, eps: float, gt: np.ndarray,
+                      rtol: float = 1e-13, maxit: int = 200000):
+    """FP64 forward + adjoint for loss = mean((alpha - gt)^2).
+
+    alpha solves (L + diag(gamma)) alpha = gamma s with L = levin_sym64(im3);
+    lam solves the same symmetric system for dloss/dalpha; the image gradient
+    back-propagates the pair gradients -(lam_i - lam_j)(alpha_i - alpha_j)
+    through the window statistics (levin_backward64) and
+    dloss/dgamma_i = lam_i (s_i - alpha_i).  Returns a dict."""
+    H, W, _ = im3.shape
+    w = levin_sym64(im3, eps)
+    g = np.asarray(gamma, np.float64).ravel()
+    sv = np.asarray(s, np.float64).ravel()
+    op = Operator(W=W, H=H, w=w, gamma=g)
+    alpha, it_a, rel_a = op.cg(g * sv, np.full(W * H, 0.5), rtol=rtol, maxit=maxit)
+    n = W * H
+    dalpha = 2.0 * (alpha - np.asarray(gt, np.float64).ravel()) / n
+    lam, it_l, rel_l = op.cg(dalpha, np.zeros(n), rtol=rtol, maxit=maxit)
+    dI = levin_backward64(sym_edge_grad(lam, alpha, W, H), im3, eps)
+    return {"alpha": alpha.reshape(H, W), "lam": lam.reshape(H, W), "dimage": dI,
+            "dgamma": (lam * (sv - alpha)).reshape(H, W), "dalpha": dalpha.reshape(H, W),
+            "loss": float(np.mean((alpha - np.asarray(gt, np.float64).ravel()) ** 2)),
+            "iters": (it_a, it_l), "rel": (rel_a, rel_l), "w": w}

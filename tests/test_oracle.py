@@ -192,3 +192,32 @@ def test_assembly_adjoint_matches_finite_differences(orc):
         im_[v, u, c] -= h
         fd = (np.sum(gw * orc.levin_sym64(ip, eps)) - np.sum(gw * orc.levin_sym64(im_, eps))) / (2 * h)
         assert abs(fd - dI[v, u, c]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_reference_adjoint_matches_full_finite_differences(orc):
+    """Solve + assembly adjoint (reference_adjoint) vs central FD of the loss,
+    each perturbed loss from a full FP64 re-solve (24x20, so it is cheap)."""
+    from gpumatting_b200.synth import make_problem
+
+    p = make_problem(24, 20, 5)
+    im = (p.image.astype(np.float32) / np.float32(255)).astype(np.float64)
+    gamma, s = p.gamma.astype(np.float64), p.s.astype(np.float64)
+    ref = orc.reference_adjoint(im, gamma, s, p.eps, p.alpha_gt)
+    h = 1e-6  # eps = 1e-5 makes the window inverse stiff: keep the O(h^2) term small
+
+    def loss(im_, gamma_):
+        r = orc.Operator(W=24, H=20, w=orc.levin_sym64(im_, p.eps), gamma=gamma_)
+        a, _, _ = r.cg((gamma_ * s).ravel(), np.full(24 * 20, 0.5), rtol=1e-14, maxit=100000)
+        return np.mean((a - p.alpha_gt.ravel()) ** 2)
+
+    for (v, u, c) in [(0, 0, 0), (5, 7, 1), (10, 12, 2), (19, 23, 0), (13, 3, 1)]:
+        ip, im_ = im.copy(), im.copy()
+        ip[v, u, c] += h
+        im_[v, u, c] -= h
+        fd = (loss(ip, gamma) - loss(im_, gamma)) / (2 * h)
+        assert abs(fd - ref["dimage"][v, u, c]) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(ref["dimage"]).max())
+        gp, gm = gamma.copy(), gamma.copy()
+        gp[v, u] += h
+        gm[v, u] -= h
+        fd = (loss(im, gp) - loss(im, gm)) / (2 * h)
+        assert abs(fd - ref["dgamma"][v, u]) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(ref["dgamma"]).max())

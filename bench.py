@@ -380,6 +380,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_fp32"] = run_plain(args, prob, img_d, scr_d, flush, stream)
         line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
+    if rank == 0 and world == 1 and args.spmv_size > 0:
+        line["spmv"] = run_spmv(args, stream, peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sweeps = calibrate_sweeps(prob, args.cpu_seconds)
         times, kind, asm = reference_cpu_path(prob, sweeps, 1, steps=1)
@@ -393,6 +395,62 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# Algorithmic bytes per pixel of one SpMV pass: band planes + diagonal plane
+# + x read once + y written once.
+SPMV_BYTES = {"fp16": 12 * 2 + 4 + 8, "bf16": 12 * 2 + 4 + 8, "fp32": 12 * 4 + 4 + 8, "true_fp32": 12 * 4 + 4 + 8,
+              "ref25": 25 * 4 + 8}
+
+
+def run_spmv(args, stream, peaks) -> dict:
+    """Standalone SpMV passes at args.spmv_size^2 (inputs larger than L2, so
+    no flush): gm_levin_apply on the FP16 store (iteration operator), on its
+    FP32 true operator, and the reference-layout 25-band FP32 gm_bm_ax."""
+    import torch
+
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
+
+    S = args.spmv_size
+    N = S * S
+    prob = make_problem(S, S, 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    img = torch.from_numpy(prob.image).to(dev)
+    scr = torch.from_numpy(prob.scribbles).to(dev)
+    out = {"size": f"{S}x{S}", "l2": "not flushed: every pass streams > 126 MB", "launches_timed": args.spmv_reps}
+
+    def time_fn(fn, k):
+        for _ in range(3):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for a, b in ev:
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return statistics.mean(a.elapsed_time(b) for a, b in ev)
+
+    st = api.LevinStore(S, S, "fp16").assemble(img, scr, eps=prob.eps, gamma_value=100.0)
+    x = torch.rand((S, S), device=dev)
+    y = torch.empty_like(x)
+    for key, true_op in (("fp16", False), ("true_fp32", True)):
+        ms = time_fn(lambda: st.apply(x, y, true_op=true_op, stream=stream), args.spmv_reps)
+        gbs = SPMV_BYTES[key] * N / (ms / 1000) / 1e9
+        out[key] = {"kernel": "gm::levin_apply_kernel", "ms": ms, "bytes_per_px": SPMV_BYTES[key],
+                    "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peaks["hbm_gbs"]}
+    del st
+    a, b = api.levin_bands25(img, scr, eps=prob.eps, gamma_value=100.0, arithmetic="fp64")
+    Lm = api.DeviceBandedMatrix(a, torch.tensor(api.levin_band_offsets(S), device=dev), N)
+    xp = api.PaddedVector(N, api.levin_pad(S))
+    xp.data.uniform_()
+    yb = torch.empty(N, device=dev)
+    ms = time_fn(lambda: api.bm_ax(yb, Lm, xp, stream=stream), args.spmv_reps)
+    gbs = SPMV_BYTES["ref25"] * N / (ms / 1000) / 1e9
+    out["ref25"] = {"kernel": "gm_bm_ax (reference 25-band FP32 layout)", "ms": ms,
+                    "bytes_per_px": SPMV_BYTES["ref25"], "achieved_gbs": gbs,
+                    "frac_of_measured_hbm": gbs / peaks["hbm_gbs"]}
+    return out
 
 
 def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
@@ -444,6 +502,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--fixed-iters", type=int, default=0, help="profiling: run exactly this many CG iterations")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--spmv-size", type=int, default=4096, help="standalone SpMV measurement size (0 = skip)")
+    ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--replace-every", type=int, default=50)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="ring configuration: 0 auto, 3 shallow, 2 deep")
     args = ap.parse_args()

@@ -103,6 +103,7 @@ SIGNATURES = {
                                        _vp]),
     "gm_default_params": (None, [C.POINTER(GmSolveParams)]),
     "gm_levin_solve": (_i, [C.POINTER(GmLevinStore), _vp, C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo), _vp]),
+    "gm_levin_apply": (_i, [C.POINTER(GmLevinStore), _vp, _i, _vp, _i, _i, _vp]),
     "gm_levin_solve_rhs": (_i, [C.POINTER(GmLevinStore), _vp, _vp, C.POINTER(GmSolveParams),
                                 C.POINTER(GmSolveInfo), _vp]),
     "gm_levin_adjoint": (_i, [C.POINTER(GmLevinStore), C.POINTER(GmImage), C.POINTER(GmScribbles), C.c_double,

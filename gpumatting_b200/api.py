@@ -289,6 +289,16 @@ class LevinStore:
         return SolveResult.from_info(info)
 
 
+    def apply(self, x, y=None, true_op: bool = False, stream=None):
+        """y = A x ([H, W'] device floats, W' >= W a multiple of 4) with the
+        iteration operator (true_op False) or the true FP32 operator."""
+        torch = _torch()
+        if y is None:
+            y = torch.empty_like(x)
+        L.check(L.load().gm_levin_apply(C.byref(self.s), x.data_ptr(), x.stride(0), y.data_ptr(), y.stride(0),
+                                        1 if true_op else 0, _stream(stream)))
+        return y
+
     def solve_rhs(self, rhs, x, solver: str = "cg", stream=None, **params) -> SolveResult:
         """Solve the store's system for rhs ([H, W] device floats); x holds the
         initial guess and receives the solution."""

@@ -254,6 +254,16 @@ void gm_default_params(gm_solve_params* p);
 int gm_levin_solve(const gm_levin_store* st, float* alpha, const gm_solve_params* p,
                    gm_solve_info* info, void* stream);
 
+/* y = A x with the store's operator in one streaming pass (the banded SpMV
+ * of BandedMatrix.cu:107-141 on the symmetric layout).  which = 0: the
+ * iteration operator of the store's precision, y_i = d_i x_i - sum_j w_ij x_j;
+ * which = 1: the true operator in FP32 planes, y_i = gamma_i x_i +
+ * sum_j w32_ij (x_i - x_j).  FP32 accumulation.  x: device [H][xpitch]
+ * floats, 16-byte aligned, xpitch a multiple of 4; y: [H][ypitch], 8-byte
+ * aligned, ypitch even. */
+int gm_levin_apply(const gm_levin_store* st, const float* x, int xpitch, float* y, int ypitch, int which,
+                   void* stream);
+
 /* Solve the store's system for another right-hand side: rhs and x are
  * device [H][W] floats (pitch W); x holds the initial guess on entry. */
 int gm_levin_solve_rhs(const gm_levin_store* st, const float* rhs, float* x, const gm_solve_params* p,

@@ -504,6 +504,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--spmv-size", type=int, default=4096, help="standalone SpMV measurement size (0 = skip)")
     ap.add_argument("--spmv-reps", type=int, default=20)
+    ap.add_argument("--spmv-only", action="store_true", help="profiling: only the standalone SpMV passes")
     ap.add_argument("--replace-every", type=int, default=50)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="ring configuration: 0 auto, 3 shallow, 2 deep")
     args = ap.parse_args()
@@ -511,6 +512,11 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.spmv_only:
+        import torch
+
+        line = {"spmv": run_spmv(args, torch.cuda.current_stream(), load_peaks())}
+        print(json.dumps(line), flush=True)
     else:
         run_ours(args)
 

@@ -47,7 +47,7 @@ class GmScribbles(C.Structure):
 class GmLevinStore(C.Structure):
     _fields_ = [("W", C.c_int), ("H", C.c_int), ("pitch", C.c_int), ("precision", C.c_int), ("w", C.c_void_p),
                 ("w32", C.c_void_p), ("gamma", C.c_void_p), ("b", C.c_void_p), ("d", C.c_void_p),
-                ("d32", C.c_void_p), ("owns", C.c_int)]
+                ("d32", C.c_void_p), ("owns", C.c_int), ("plane_stride", C.c_size_t)]
 
 
 class GmSolveParams(C.Structure):
@@ -103,6 +103,14 @@ SIGNATURES = {
                                        _vp]),
     "gm_default_params": (None, [C.POINTER(GmSolveParams)]),
     "gm_levin_solve": (_i, [C.POINTER(GmLevinStore), _vp, C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo), _vp]),
+    "gm_batch_create": (_i, [C.POINTER(C.c_void_p), _i, C.POINTER(C.c_int), C.POINTER(C.c_int), _i]),
+    "gm_batch_destroy": (_i, [_vp]),
+    "gm_batch_store": (_i, [_vp, _i, C.POINTER(GmLevinStore)]),
+    "gm_batch_assemble": (_i, [_vp, _i, C.POINTER(GmImage), C.POINTER(GmScribbles), C.c_double, _vp]),
+    "gm_batch_tune": (_i, [_vp, C.POINTER(GmSolveParams), _i, _vp]),
+    "gm_batch_solve": (_i, [_vp, C.POINTER(C.c_void_p), C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo), _vp]),
+    "gm_batch_info": (_i, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                           C.POINTER(C.c_int)]),
     "gm_levin_apply": (_i, [C.POINTER(GmLevinStore), _vp, _i, _vp, _i, _i, _vp]),
     "gm_levin_solve_rhs": (_i, [C.POINTER(GmLevinStore), _vp, _vp, C.POINTER(GmSolveParams),
                                 C.POINTER(GmSolveInfo), _vp]),

@@ -336,6 +336,66 @@ class LevinStore:
         return dimage, dgamma, lam, SolveResult.from_info(info)
 
 
+class LevinBatch:
+    """gm_batch: many images of different sizes solved in one persistent
+    launch (replayed from a CUDA graph), with a tuned launch shape."""
+
+    def __init__(self, sizes, precision: str = "fp16"):
+        self.sizes = [(int(w), int(h)) for w, h in sizes]
+        n = len(self.sizes)
+        ws = (C.c_int * n)(*[w for w, _ in self.sizes])
+        hs = (C.c_int * n)(*[h for _, h in self.sizes])
+        self.h = C.c_void_p()
+        L.check(L.load().gm_batch_create(C.byref(self.h), n, ws, hs, PRECISIONS[precision]))
+        self.precision = precision
+        self._inputs = [None] * n
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.load().gm_batch_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.sizes)
+
+    def assemble(self, k: int, image, scribbles=None, eps: float = 1e-5, gamma_value: float = 100.0, gamma_map=None,
+                 s_map=None, stream=None):
+        im = _image_desc(image)
+        sc = _scrib_desc(scribbles, gamma_value, gamma_map, s_map)
+        L.check(L.load().gm_batch_assemble(self.h, k, C.byref(im), C.byref(sc), eps, _stream(stream)))
+        self._inputs[k] = (image, scribbles, gamma_map, s_map)
+        return self
+
+    def store_view(self, k: int) -> L.GmLevinStore:
+        v = L.GmLevinStore()
+        L.check(L.load().gm_batch_store(self.h, k, C.byref(v)))
+        return v
+
+    def tune(self, iters: int = 20, stream=None, **params) -> dict:
+        p = L.default_params(**params)
+        L.check(L.load().gm_batch_tune(self.h, C.byref(p), iters, _stream(stream)))
+        return self.info()
+
+    def info(self) -> dict:
+        v = [C.c_int() for _ in range(5)]
+        L.check(L.load().gm_batch_info(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(["ctas_per_sm", "ring_cfg", "row_mult", "graph_launches", "grid"], [x.value for x in v]))
+
+    def solve(self, alphas, solver: str = "cg", stream=None, **params) -> list:
+        n = len(self.sizes)
+        assert len(alphas) == n
+        ptrs = (C.c_void_p * n)(*[a.data_ptr() for a in alphas])
+        infos = (L.GmSolveInfo * n)()
+        p = L.default_params(solver=SOLVERS[solver], **params)
+        rc = L.load().gm_batch_solve(self.h, ptrs, C.byref(p), infos, _stream(stream))
+        if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
+            L.check(rc)
+        return [SolveResult.from_info(infos[k]) for k in range(n)]
+
+
 class _CudaArray:
     """Minimal __cuda_array_interface__ holder so torch can view device
     memory that libgpumat owns (no copy)."""

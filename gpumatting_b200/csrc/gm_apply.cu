@@ -253,7 +253,8 @@ extern "C" int gm_levin_apply(const gm_levin_store* stv, const float* x, int xpi
     CUtensorMap mw, mx, md;
     {
         const uint64_t d3[3] = {(uint64_t)W, (uint64_t)H, 12};
-        const uint64_t s3[2] = {(uint64_t)P * es, (uint64_t)H * P * es};
+        const uint64_t ps = stv->plane_stride ? (uint64_t)stv->plane_stride : (uint64_t)H * P;
+        const uint64_t s3[2] = {(uint64_t)P * es, ps * es};
         const uint32_t b3[3] = {(uint32_t)kApplyBoxW, (uint32_t)(th + 2), 12};
         GM_TRY(gm_make_tmap(&mw, dt, 3, const_cast<void*>(wbase), d3, s3, b3));
     }

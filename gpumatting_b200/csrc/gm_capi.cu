@@ -138,7 +138,8 @@ static int levin_solve_impl(const gm_levin_store* store, const float* b, int bpi
     hi.esize = 4;
     hi.base = store->w32;
     hi.row_stride = (uint64_t)P * 4;
-    hi.plane_stride = (uint64_t)H * P * 4;
+    const uint64_t pstride = store->plane_stride ? (uint64_t)store->plane_stride : (uint64_t)H * P;
+    hi.plane_stride = pstride * 4;
     hi.planes = 12;
     OpSource lo = hi;
     lo.kind = OP_SYMD;
@@ -148,7 +149,7 @@ static int levin_solve_impl(const gm_levin_store* store, const float* b, int bpi
         lo.esize = 2;
         lo.base = store->w;
         lo.row_stride = (uint64_t)P * 2;
-        lo.plane_stride = (uint64_t)H * P * 2;
+        lo.plane_stride = pstride * 2;
     }
     S.lo = lo;
     S.hi = hi;

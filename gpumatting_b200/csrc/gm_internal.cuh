@@ -396,6 +396,102 @@ __device__ __forceinline__ bool grid_allreduce(GridBarrier* gb, double* parts, u
     return s_ok != 0;
 }
 
+// Batched form of grid_allreduce: components 0 .. NV-2 are summed over the
+// CTAs lo .. hi-1 only (the CTAs of one image; lo == hi gives zeros) and
+// component NV-1 over the whole grid.  Same barrier, same fixed order, so
+// the CTAs of one image agree bit for bit.
+template <int NV>
+__device__ __forceinline__ bool grid_allreduce_seg(GridBarrier* gb, double* parts, unsigned G, int lo, int hi,
+                                                   uint64_t limit_ns, double (&v)[NV], double* scratch)
+{
+    __shared__ int s_ok;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) scratch[wid * NV + k] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        double cs[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? scratch[lane * NV + k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            cs[k] = x;
+        }
+        int ok = 1;
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) parts[(size_t)k * G + blockIdx.x] = cs[k];
+            const unsigned g = ld_acquire(&gb->gen);
+            const unsigned arrived = atom_add_acq_rel(&gb->count, 1u);
+            if (arrived == G - 1) {
+                gb->count = 0;
+                st_release(&gb->gen, g + 1);
+            } else {
+                uint64_t t0 = 0;
+                unsigned spins = 0;
+                while (ld_acquire(&gb->gen) == g) {
+                    ++spins;
+                    if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) { ok = 0; break; }
+                    if ((spins & 63u) == 0) {
+                        const uint64_t now = globaltimer_ns();
+                        if (t0 == 0) t0 = now;
+                        else if (now - t0 > limit_ns) {
+                            atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
+                            atomicExch(&gb->where, 1);
+                            ok = 0;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) {
+            double a[NV], b[NV];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) { a[k] = 0.0; b[k] = 0.0; }
+            int i = lo + lane;
+            for (; i + 32 < hi; i += 64) {
+#pragma unroll
+                for (int k = 0; k < NV - 1; ++k) {
+                    a[k] += __ldcg(parts + (size_t)k * G + i);
+                    b[k] += __ldcg(parts + (size_t)k * G + i + 32);
+                }
+            }
+            if (i < hi) {
+#pragma unroll
+                for (int k = 0; k < NV - 1; ++k) a[k] += __ldcg(parts + (size_t)k * G + i);
+            }
+            const double* pl = parts + (size_t)(NV - 1) * G;
+            i = lane;
+            for (; i + 32 < (int)G; i += 64) {
+                a[NV - 1] += __ldcg(pl + i);
+                b[NV - 1] += __ldcg(pl + i + 32);
+            }
+            if (i < (int)G) a[NV - 1] += __ldcg(pl + i);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                double x = a[k] + b[k];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+                if (lane == 0) scratch[32 * NV + k] = x;
+            }
+        }
+        if (lane == 0) s_ok = ok;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = scratch[32 * NV + k];
+    return s_ok != 0;
+}
+
 template <class T> struct Cvt;
 template <> struct Cvt<float> {
     static __device__ __forceinline__ float to_f(float x) { return x; }

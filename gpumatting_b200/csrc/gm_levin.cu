@@ -100,6 +100,7 @@ struct SymOut {
     float* gamma;     // [H][pitch]
     float* b;         // [H][pitch]
     int pitch;
+    size_t plane;     // elements between planes of w / w32
     float* a25;       // optional [25][apitch]
     size_t apitch;
     float* b25;       // optional [N]
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(TW * TH) levin_sym_kernel(ImgView im, ScribVie
     }
     float gam, bv;
     scribble(sc, u, v, gam, bv);
-    const size_t plane = (size_t)H * o.pitch;
+    const size_t plane = o.plane;
     const size_t gi = (size_t)v * o.pitch + u;
     T* wl = reinterpret_cast<T*>(o.w);
 #pragma unroll
@@ -331,11 +332,11 @@ __global__ void __launch_bounds__(TW * TH) levin_ref_kernel(ImgView im, ScribVie
 // low-precision planes (d) and the FP32 planes (d32).
 template <class T>
 __global__ void levin_diag_kernel(const T* __restrict__ w, const float* __restrict__ w32,
-                                  const float* __restrict__ gamma, float* d, float* d32, int W, int H, int pitch)
+                                  const float* __restrict__ gamma, float* d, float* d32, int W, int H, int pitch,
+                                  size_t plane)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     if (u >= W) return;
-    const size_t plane = (size_t)H * pitch;
     const size_t i = (size_t)v * pitch + u;
     double s = gamma[i], s32 = gamma[i];
 #pragma unroll
@@ -361,7 +362,8 @@ static void launch_sym(const ImgView& im, const ScribView& sc, double eps, int W
     dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH);
     levin_sym_kernel<T><<<grid, TW * TH, 0, st>>>(im, sc, eps, W, H, o);
     dim3 g2((W + 127) / 128, H);
-    levin_diag_kernel<T><<<g2, 128, 0, st>>>(reinterpret_cast<const T*>(o.w), o.w32, o.gamma, d, d32, W, H, o.pitch);
+    levin_diag_kernel<T><<<g2, 128, 0, st>>>(reinterpret_cast<const T*>(o.w), o.w32, o.gamma, d, d32, W, H, o.pitch,
+                                             o.plane);
 }
 
 // ---------------------------------------------------------------------------
@@ -583,6 +585,7 @@ extern "C" int gm_levin_assemble(gm_levin_store* st, const gm_image* im, const g
     o.gamma = st->gamma;
     o.b = st->b;
     o.pitch = st->pitch;
+    o.plane = st->plane_stride ? st->plane_stride : (size_t)st->H * st->pitch;
     if (bands25) {
         if (!bands25->a || bands25->nbands != 25 || bands25->rows != st->W * st->H ||
             bands25->apitch < (size_t)bands25->rows) {

@@ -247,8 +247,8 @@ __device__ __forceinline__ void load_rows(V (&X)[6][6], const V* ring, int r0, i
 }
 
 template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, int KIND>
-__device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* smem, int u0, int v0, int v1,
-                                          const KState& s, double (&part)[kNPart], Pipe& pp)
+__device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& geo, unsigned char* smem, int u0,
+                                          int v0, int v1, const KState& s, double (&part)[kNPart], Pipe& pp)
 {
     constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED, CFG);
     constexpr KindLayout K = L.k[KIND];
@@ -333,7 +333,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     const int c = 8 + kWarpCols * w + 2 * lane;        // smem column of this lane's pixel pair
     const int lc0 = 2 * lane;                          // first operand column (local ring index)
     const int u = u0 + kWarpCols * w + 2 * lane;       // image column of pixel 0
-    const bool in0 = u < A.W, in1 = u + 1 < A.W;
+    const bool in0 = u < geo.W, in1 = u + 1 < geo.W;
     // extra operand pair for the ring halo: lane 0 left, lane 1 right
     const bool has_x = lane < 2;
     const int cx = lane == 0 ? 6 + kWarpCols * w : 8 + kWarpCols * w + kWarpCols;
@@ -564,7 +564,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
                     }
                     auto rep_row = [&](double y0, double y1, const float2 bv, size_t g, int vr, int ro) {
                         const float r0f = (float)((double)bv.x - y0), r1f = (float)((double)bv.y - y1);
-                        float* ao = A.alpha_out + (size_t)vr * A.alpha_pitch + u;
+                        float* ao = geo.aout + (size_t)(vr - geo.arow0) * geo.apitch + u;
                         ao[0] = (float)X[ro + 2][2];
                         A.r[s.c][g] = r0f;
                         part[0] += (double)r0f * (double)r0f;
@@ -624,7 +624,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, unsigned char* sm
     release_bands_to(nband);
 }
 
-template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG>
+template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, bool BATCH>
 __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant__ SolverArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -634,13 +634,35 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     double* red = reinterpret_cast<double*>(smem + L.red_off);
 
-    const int unit = blockIdx.x;
-    int u0 = 0, v0 = 0, v1 = 0;
-    if (unit < A.nunits) {
-        const int st = unit % A.nstrips, sg = unit / A.nstrips;
-        u0 = st * kStrip;
-        v0 = (int)((long long)A.H * sg / A.nseg);
-        v1 = (int)((long long)A.H * (sg + 1) / A.nseg);
+    // This CTA's unit: a 192-column strip of a row segment of one image.
+    int img = -1, u0 = 0, v0 = 0, v1 = 0, lo = 0, hi = 0;
+    UnitGeo geo;
+    if constexpr (BATCH) {
+        geo.W = 0; geo.arow0 = 0; geo.apitch = 0; geo.aout = nullptr; geo.ain = nullptr;
+        const int b = blockIdx.x;
+        for (int k = 0; k < A.nimg; ++k) {
+            const BatchImage I = A.imgs[k];
+            if (b >= I.c0 && b < I.c0 + I.units) {
+                img = k;
+                const int unit = b - I.c0;
+                const int st = unit % I.nstrips, sg = unit / I.nstrips;
+                u0 = st * kStrip;
+                v0 = I.y0 + (int)((long long)I.H * sg / I.nseg);
+                v1 = I.y0 + (int)((long long)I.H * (sg + 1) / I.nseg);
+                lo = I.c0;
+                hi = I.c0 + I.units;
+                geo.W = I.W; geo.arow0 = I.y0; geo.apitch = I.W; geo.aout = I.alpha; geo.ain = I.alpha;
+            }
+        }
+    } else {
+        const int unit = blockIdx.x;
+        if (unit < A.nunits) {
+            const int st = unit % A.nstrips, sg = unit / A.nstrips;
+            u0 = st * kStrip;
+            v0 = (int)((long long)A.H * sg / A.nseg);
+            v1 = (int)((long long)A.H * (sg + 1) / A.nseg);
+        }
+        geo.W = A.W; geo.arow0 = 0; geo.apitch = A.alpha_pitch; geo.aout = A.alpha_out; geo.ain = A.alpha_in;
     }
     const bool active = v1 > v0;
 
@@ -662,9 +684,9 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
         for (int v = v0; v < v1; ++v)
             for (int cl = tid; cl < kStrip; cl += blockDim.x) {
                 const int u = u0 + cl;
-                if (u >= A.W) continue;
+                if (u >= geo.W) continue;
                 const size_t i = (size_t)v * A.P + u;
-                const float a0 = A.alpha_in[(size_t)v * A.alpha_pitch + u];
+                const float a0 = geo.ain[(size_t)(v - geo.arow0) * geo.apitch + u];
                 if (MIXED) {
                     A.base[0][i] = jac ? 0.0 : (double)a0;
                     A.base[1][i] = 0.0;
@@ -690,26 +712,49 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
         kind = KIND_REPLACE;
         final_rep = true;
     }
+    // Batched solves: a CTA whose image has converged (or that has no image)
+    // keeps joining the grid barrier with no work until every image is done.
+    bool done = BATCH && img < 0;
 
     while (ok) {
         double part[kNPart] = {0.0, 0.0, 0.0, 0.0};
-        if (active) {
+        if (active && !done) {
             if (kind == KIND_KRYLOV)
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, geo, smem, u0, v0, v1, s, part, pp);
             else if (kind == KIND_REPLACE)
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_REPLACE>(A, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_REPLACE>(A, geo, smem, u0, v0, v1, s, part, pp);
             else
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, geo, smem, u0, v0, v1, s, part, pp);
         }
-        ok = grid_allreduce<kNPart>(A.gb, A.partials + (size_t)parity * G * kNPart, G, A.limit_ns, part, red);
-        if (!ok) break;
+        if constexpr (BATCH) {
+            double v5[kNPart + 1] = {part[0], part[1], part[2], part[3], done ? 0.0 : 1.0};
+            ok = grid_allreduce_seg<kNPart + 1>(A.gb, A.partials + (size_t)parity * G * (kNPart + 1), G, lo, hi,
+                                                A.limit_ns, v5, red);
+            if (!ok) break;
+#pragma unroll
+            for (int k = 0; k < kNPart; ++k) part[k] = v5[k];
+            parity ^= 1;
+            if (!(v5[kNPart] > 0.0)) break;  // no CTA worked in this sweep: every image is done
+            if (done) continue;
+        } else {
+            ok = grid_allreduce<kNPart>(A.gb, A.partials + (size_t)parity * G * kNPart, G, A.limit_ns, part, red);
+            if (!ok) break;
+            parity ^= 1;
+        }
         const double (&tot)[kNPart] = part;
-        parity ^= 1;
 
         if (kind == KIND_KRYLOV) {
             s.c ^= 1;
             ++it;
             const double rr = tot[0], pq = tot[1], rq = tot[2], qq = tot[3];
+            if (isfinite(rr) && !(rr > 1e-32 * bb)) {
+                // residual at the end of FP64 precision (exactly 0 on tiny
+                // systems iterated with rtol = 0): converged, not broken down
+                s.ad = 0.0; s.af = 0.f;
+                kind = KIND_REPLACE;
+                final_rep = true;
+                continue;
+            }
             if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) {
                 status = GM_ERR_BREAKDOWN;
                 s.ad = 0.0; s.af = 0.f;
@@ -746,7 +791,14 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
             rr_true = tot[0];
             rel = sqrt(rr_true / bb);
             if (!isfinite(rr_true)) status = GM_ERR_BREAKDOWN;
-            if (final_rep || (A.rtol > 0.0 && rel <= A.rtol) || it >= A.max_iters || !isfinite(rr_true)) break;
+            if (final_rep || (A.rtol > 0.0 && rel <= A.rtol) || it >= A.max_iters || !isfinite(rr_true)) {
+                if constexpr (BATCH) {
+                    done = true;
+                    continue;
+                } else {
+                    break;
+                }
+            }
             const bool bz = restart_due || gd || !(rr_prev > 0.0);
             const double be = bz ? 0.0 : rr_true / rr_prev;
             s.bf = (float)be;
@@ -771,17 +823,19 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
             }
         }
     }
-    if (blockIdx.x == 0 && tid == 0) {
+    const bool reporter = BATCH ? (img >= 0 && (int)blockIdx.x == lo) : blockIdx.x == 0;
+    if (reporter && tid == 0) {
+        SolverOut* o = BATCH ? A.outs + img : A.out;
         const int ab = ld_volatile_int(&A.gb->abort);
         if (ab) status = ab;
         else if (status == GM_OK && A.rtol > 0.0 && !(rel <= A.rtol)) status = GM_ERR_NOT_CONVERGED;
-        A.out->status = status;
-        A.out->iters = it;
-        A.out->replacements = nrep;
-        A.out->where = A.gb->where;
-        A.out->rr_true = rr_true;
-        A.out->bb = bb;
-        A.out->rel = rel;
+        o->status = status;
+        o->iters = it;
+        o->replacements = nrep;
+        o->where = A.gb->where;
+        o->rr_true = rr_true;
+        o->bb = bb;
+        o->rel = rel;
     }
     __syncthreads();
     if (tid == 0)
@@ -797,3 +851,4 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
 // Host driver
 // ---------------------------------------------------------------------------
 #include "gm_solver_host.inc"
+#include "gm_batch_host.inc"

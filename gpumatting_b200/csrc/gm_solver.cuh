@@ -21,7 +21,7 @@ constexpr int kRingCols = kWarpCols + 4;         // private operand ring: warp c
 constexpr int kRvMax = 16;                       // vector ring slots
 constexpr int kRbMax = 16;                       // band ring slots
 constexpr int kNPart = 4;                        // FP64 partial sums per CTA per sweep
-constexpr int kRedBytes = (32 + 1) * kNPart * 8;  // reduction scratch: warp sums + grid totals
+constexpr int kRedBytes = (32 + 1) * (kNPart + 1) * 8;  // reduction scratch: warp sums + grid totals
 
 // Shared-memory carve of one sweep kind.  Everything here is a compile-time
 // function of the operator types, so the hot loop indexes rings with
@@ -129,6 +129,28 @@ struct SolverOut {
     double rel;
 };
 
+// One image of a batched solve.  Images are stacked in one canvas, image k
+// occupying canvas rows y0 .. y0+H-1 (columns 0 .. W-1) with two zero rows
+// between neighbours; its units are CTAs c0 .. c0+units-1 (nstrips strips x
+// nseg row segments).
+struct BatchImage {
+    int y0, W, H;
+    int nstrips, nseg;
+    int c0, units;
+    int pad_;
+    float* alpha;             // [H][W] device: initial guess in, solution out
+};
+
+// Where a CTA's unit lives: image width for masking, and where its solution
+// rows go (row vr of the canvas is row vr - arow0 of aout).
+struct UnitGeo {
+    int W;
+    int arow0;
+    int apitch;
+    float* aout;
+    const float* ain;
+};
+
 struct SolverArgs {
     // Tensor maps: vectors are 2-D {W, H}; bands 3-D {W, H, planes}.
     CUtensorMap m_r[2], m_q[2], m_p[2], m_xacc[2], m_base[2];
@@ -160,6 +182,10 @@ struct SolverArgs {
     uint64_t limit_ns;       // grid-barrier wait limit
     uint64_t tma_limit_ns;   // TMA / ring wait limit (never below 2 s)
     int inject;              // 1: first grid barrier expects one extra arrival
+    // batched solves (BATCH kernels only)
+    const BatchImage* imgs;
+    int nimg;
+    SolverOut* outs;         // [nimg]
 };
 
 }  // namespace gm

@@ -201,6 +201,9 @@ typedef struct gm_levin_store_s {
     float* d;             /* [H][pitch] gamma + row sum of w               */
     float* d32;           /* [H][pitch] gamma + row sum of w32             */
     int owns;             /* set by gm_levin_store_alloc                  */
+    size_t plane_stride;  /* elements between consecutive planes of w and
+                             w32; 0 means H * pitch (a view into a larger
+                             canvas, as batched stores use, sets it)       */
 } gm_levin_store;
 
 int gm_levin_store_alloc(gm_levin_store* st, int W, int H, int precision);
@@ -285,6 +288,37 @@ int gm_levin_adjoint(const gm_levin_store* st, const gm_image* im, const gm_scri
                      const float* alpha, const float* dalpha, float* lambda, float* dimage,
                      size_t dimage_pitch, int dimage_channels, float* dgamma, const gm_solve_params* p,
                      gm_solve_info* info, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Batched solves: many images of different sizes in one persistent   */
+/* launch (no counterpart in the reference, which solves one image).   */
+/* ------------------------------------------------------------------ */
+typedef struct gm_batch_s gm_batch;
+
+/* Allocates one canvas store + work vectors for `count` images of the given
+ * sizes (stacked, 2 zero rows apart) in `precision`; everything zeroed. */
+int gm_batch_create(gm_batch** b, int count, const int* widths, const int* heights, int precision);
+int gm_batch_destroy(gm_batch* b);
+/* View of image k's planes inside the canvas (plane_stride set; owns = 0):
+ * usable with gm_levin_assemble, gm_levin_apply, gm_levin_solve. */
+int gm_batch_store(const gm_batch* b, int k, gm_levin_store* view);
+/* gm_levin_assemble into image k's view. */
+int gm_batch_assemble(gm_batch* b, int k, const gm_image* im, const gm_scribbles* sc, double eps,
+                      void* stream);
+/* Times the candidate launch shapes (ring configuration x CTAs per SM x
+ * rows per unit) for `iters` fixed iterations each and keeps the fastest. */
+int gm_batch_tune(gm_batch* b, const gm_solve_params* p, int iters, void* stream);
+/* Solves every image in one cooperative launch, replayed from a CUDA graph
+ * captured on first use (recaptured when the parameters or the shape
+ * change).  alphas: host array of `count` device pointers ([H_k][W_k],
+ * initial guess in, solution out); infos: `count` results (kernel_ms and
+ * grid are those of the one launch).  p->ctas_per_sm = 0 uses the tuned
+ * shape (tuning on first use).  Returns the worst per-image status. */
+int gm_batch_solve(gm_batch* b, float* const* alphas, const gm_solve_params* p, gm_solve_info* infos,
+                   void* stream);
+/* Tuned shape (0 / -1 before tuning), graph launches so far, last grid. */
+int gm_batch_info(const gm_batch* b, int* tuned_ctas_per_sm, int* tuned_ring_cfg, int* tuned_row_mult,
+                  int* graph_launches, int* grid);
 
 /* Solve with a 25-band BandedMatrix on the device (reference layout).
  * W > 0 declares the Levin stencil of an image W wide (rows = W*H) and

@@ -375,11 +375,13 @@ def run_ours(args):
                          "kernel": "gm::solver_kernel (fused persistent CG)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * (3 + 1 + 4),
                     "d2h_bytes_per_step": N * 4, "ms_per_step": 1000 * te_max / args.steps},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 3 * args.steps,  # per step: levin_sym_kernel, levin_diag_kernel, solver_kernel
             "clocks": clk}
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_fp32"] = run_plain(args, prob, img_d, scr_d, flush, stream)
         line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
+    if rank == 0 and world == 1 and args.batch_count > 0:
+        line["batch"] = run_batch(args, stream)
     if rank == 0 and world == 1 and args.spmv_size > 0:
         line["spmv"] = run_spmv(args, stream, peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -453,6 +455,70 @@ def run_spmv(args, stream, peaks) -> dict:
     return out
 
 
+def run_batch(args, stream) -> dict:
+    """64 images, W and H uniform in [256, 1024] (seeded): all assembled into
+    one FP16 batch store and solved to rel-res 1e-6 in ONE persistent launch
+    replayed from a CUDA graph (launch shape from the batch autotuner), versus
+    the same 64 images solved one after another with the plain FP32 method
+    (25-band FP32 store, fused CG to 1e-6)."""
+    import torch
+
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import batch_sizes, make_problem
+
+    sizes = batch_sizes(args.batch_count, 256, 1024, seed=0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    probs = [make_problem(W, H, 100 + k) for k, (W, H) in enumerate(sizes)]
+    imgs = [torch.from_numpy(p.image).to(dev) for p in probs]
+    scrs = [torch.from_numpy(p.scribbles).to(dev) for p in probs]
+    npx = sum(W * H for W, H in sizes)
+    batch = api.LevinBatch(sizes, "fp16")
+    for k, p in enumerate(probs):
+        batch.assemble(k, imgs[k], scrs[k], eps=p.eps, gamma_value=100.0, stream=stream)
+    alphas = [torch.empty((H, W), device=dev) for W, H in sizes]
+    t_tune = time.time()
+    shape = batch.tune(iters=20, stream=stream)
+    t_tune = time.time() - t_tune
+    ms, res = [], None
+    for i in range(2 + args.batch_steps):
+        for a in alphas:
+            a.fill_(0.5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = batch.solve(alphas, "cg", rtol=1e-6, max_iters=5000, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            ms.append(e0.elapsed_time(e1))
+    assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res), [r.status for r in res]
+    its = [r.iters for r in res]
+    batch_ms = statistics.mean(ms)
+    # sequential plain FP32 solves of the same images
+    seq_ms, seq_its = 0.0, []
+    for k, p in enumerate(probs):
+        W, H = sizes[k]
+        a, b = api.levin_bands25(imgs[k], scrs[k], eps=p.eps, gamma_value=100.0, arithmetic="fp64")
+        Lm = api.DeviceBandedMatrix(a, torch.tensor(api.levin_band_offsets(W), device=dev), W * H)
+        x = api.PaddedVector(W * H, api.levin_pad(W))
+        for rep in range(2):
+            x.data.fill_(0.5)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = api.banded_solve(Lm, x, b, W=W, solver="cg", rtol=1e-6, max_iters=5000, replace_every=50)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        assert r.status == 0, r
+        seq_ms += e0.elapsed_time(e1)
+        seq_its.append(r.iters)
+        del a, b, Lm, x
+    return {"images": len(sizes), "mpix": npx / 1e6, "sizes": "W, H uniform in [256, 1024], seed 0",
+            "batch_ms": batch_ms, "batch_mpix_iter_s": sum(W * H * i for (W, H), i in zip(sizes, its)) / 1e3 / batch_ms,
+            "iters_min_mean_max": [min(its), statistics.mean(its), max(its)],
+            "launch": "1 cooperative launch from a CUDA graph", "tuned_shape": shape, "tune_s": t_tune,
+            "sequential_plain_fp32_ms": seq_ms, "sequential_iters_mean": statistics.mean(seq_its),
+            "speedup_vs_sequential_plain": seq_ms / batch_ms}
+
+
 def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
     """Plain FP32 method: 25-band FP32 store + fused CG to 1e-6."""
     import numpy as np
@@ -505,6 +571,9 @@ def main():
     ap.add_argument("--spmv-size", type=int, default=4096, help="standalone SpMV measurement size (0 = skip)")
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--spmv-only", action="store_true", help="profiling: only the standalone SpMV passes")
+    ap.add_argument("--batch-count", type=int, default=64, help="batched-solve measurement: images (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--batch-only", action="store_true", help="profiling: only the batched solve")
     ap.add_argument("--replace-every", type=int, default=50)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="ring configuration: 0 auto, 3 shallow, 2 deep")
     args = ap.parse_args()
@@ -512,6 +581,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.batch_only:
+        import torch
+
+        print(json.dumps({"batch": run_batch(args, torch.cuda.current_stream())}), flush=True)
     elif args.spmv_only:
         import torch
 

@@ -129,25 +129,15 @@ def dist_setup():
 
 
 def allreduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from gpumatting_b200.shard import max_over_ranks
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return x if world == 1 else max_over_ranks(x)
 
 
 def allreduce_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from gpumatting_b200.shard import sum_over_ranks
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return x if world == 1 else sum_over_ranks(x)
 
 
 def barrier(world: int):
@@ -380,8 +370,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_fp32"] = run_plain(args, prob, img_d, scr_d, flush, stream)
         line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
-    if rank == 0 and world == 1 and args.batch_count > 0:
-        line["batch"] = run_batch(args, stream)
+    if args.batch_count > 0:
+        line["batch"] = run_batch(args, stream, world, rank)
     if rank == 0 and world == 1 and args.spmv_size > 0:
         line["spmv"] = run_spmv(args, stream, peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -455,7 +445,7 @@ def run_spmv(args, stream, peaks) -> dict:
     return out
 
 
-def run_batch(args, stream) -> dict:
+def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
     """64 images, W and H uniform in [256, 1024] (seeded): all assembled into
     one FP16 batch store and solved to rel-res 1e-6 in ONE persistent launch
     replayed from a CUDA graph (launch shape from the batch autotuner), versus
@@ -466,9 +456,13 @@ def run_batch(args, stream) -> dict:
     from gpumatting_b200 import api
     from gpumatting_b200.synth import batch_sizes, make_problem
 
-    sizes = batch_sizes(args.batch_count, 256, 1024, seed=0)
+    from gpumatting_b200.shard import shard_images
+
+    all_sizes = batch_sizes(args.batch_count, 256, 1024, seed=0)
+    mine = shard_images(all_sizes, world)[rank]  # whole images per rank, no exchange
+    sizes = [all_sizes[k] for k in mine]
     dev = torch.device("cuda", torch.cuda.current_device())
-    probs = [make_problem(W, H, 100 + k) for k, (W, H) in enumerate(sizes)]
+    probs = [make_problem(W, H, 100 + k) for k, (W, H) in zip(mine, sizes)]
     imgs = [torch.from_numpy(p.image).to(dev) for p in probs]
     scrs = [torch.from_numpy(p.scribbles).to(dev) for p in probs]
     npx = sum(W * H for W, H in sizes)
@@ -492,7 +486,16 @@ def run_batch(args, stream) -> dict:
             ms.append(e0.elapsed_time(e1))
     assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res), [r.status for r in res]
     its = [r.iters for r in res]
-    batch_ms = statistics.mean(ms)
+    batch_ms = allreduce_max(statistics.mean(ms), world)
+    work = allreduce_sum(sum(W * H * i for (W, H), i in zip(sizes, its)), world)
+    npx = allreduce_sum(npx, world)
+    out = {"images": len(all_sizes), "n_gpus": world, "mpix": npx / 1e6,
+           "sizes": "W, H uniform in [256, 1024], seed 0; size-balanced bins of whole images per GPU",
+           "batch_ms": batch_ms, "batch_mpix_iter_s": work / 1e3 / batch_ms,
+           "iters_min_mean_max": [min(its), statistics.mean(its), max(its)],
+           "launch": "1 cooperative launch per GPU from a CUDA graph", "tuned_shape": shape, "tune_s": t_tune}
+    if world > 1:
+        return out
     # sequential plain FP32 solves of the same images
     seq_ms, seq_its = 0.0, []
     for k, p in enumerate(probs):
@@ -511,12 +514,9 @@ def run_batch(args, stream) -> dict:
         seq_ms += e0.elapsed_time(e1)
         seq_its.append(r.iters)
         del a, b, Lm, x
-    return {"images": len(sizes), "mpix": npx / 1e6, "sizes": "W, H uniform in [256, 1024], seed 0",
-            "batch_ms": batch_ms, "batch_mpix_iter_s": sum(W * H * i for (W, H), i in zip(sizes, its)) / 1e3 / batch_ms,
-            "iters_min_mean_max": [min(its), statistics.mean(its), max(its)],
-            "launch": "1 cooperative launch from a CUDA graph", "tuned_shape": shape, "tune_s": t_tune,
-            "sequential_plain_fp32_ms": seq_ms, "sequential_iters_mean": statistics.mean(seq_its),
-            "speedup_vs_sequential_plain": seq_ms / batch_ms}
+    out.update({"sequential_plain_fp32_ms": seq_ms, "sequential_iters_mean": statistics.mean(seq_its),
+                "speedup_vs_sequential_plain": seq_ms / batch_ms})
+    return out
 
 
 def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:

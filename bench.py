@@ -372,6 +372,8 @@ def run_ours(args):
         line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
     if args.batch_count > 0:
         line["batch"] = run_batch(args, stream, world, rank)
+    if rank == 0 and world == 1 and args.large_size > 0:
+        line["large"] = run_large(args, stream, peaks)
     if rank == 0 and world == 1 and args.spmv_size > 0:
         line["spmv"] = run_spmv(args, stream, peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -395,6 +397,71 @@ SPMV_BYTES = {"fp16": 12 * 2 + 4 + 8, "bf16": 12 * 2 + 4 + 8, "fp32": 12 * 4 + 4
               "ref25": 25 * 4 + 8}
 
 
+_PROBLEMS = {}
+
+
+def cached_problem(W: int, H: int, seed: int):
+    from gpumatting_b200.synth import make_problem
+
+    key = (W, H, seed)
+    if key not in _PROBLEMS:
+        _PROBLEMS[key] = make_problem(W, H, seed)
+    return _PROBLEMS[key]
+
+
+def run_large(args, stream, peaks) -> dict:
+    """The large single solve: args.large_size^2 (generator smoothing x4,
+    ~5 % scribbles, eps 1e-7), FP16 store, mixed CG to rel-res 1e-6 from
+    alpha = 0.5, then the adjoint of loss = mean((alpha - alpha_gt)^2) (one
+    more solve for lambda + the window back-propagation)."""
+    import numpy as np
+    import torch
+
+    from gpumatting_b200 import api
+
+    S = args.large_size
+    N = S * S
+    prob = cached_problem(S, S, 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    img = torch.from_numpy(prob.image).to(dev)
+    scr = torch.from_numpy(prob.scribbles).to(dev)
+    gt = torch.from_numpy(prob.alpha_gt.astype(np.float32)).to(dev)
+    st = api.LevinStore(S, S, "fp16")
+    alpha = torch.empty((S, S), device=dev)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    out = {"size": f"{S}x{S}", "eps": prob.eps, "precision": "fp16"}
+    for rep in range(2):  # the first run warms caches and the workspace
+        e0, e1 = ev()
+        e0.record(stream)
+        st.assemble(img, scr, eps=prob.eps, gamma_value=100.0, stream=stream)
+        e1.record(stream)
+        alpha.fill_(0.5)
+        r = st.solve(alpha, "cg", rtol=1e-6, max_iters=5000, stream=stream)
+        torch.cuda.synchronize()
+    alg = N * (r.iters * KRYLOV_BYTES["fp16"] + r.replacements * REPLACE_BYTES["sym_mixed"]
+               + IMPORT_BYTES["sym_mixed"])
+    out.update({"assemble_ms": e0.elapsed_time(e1), "solve_status": r.status, "iters": r.iters,
+                "replacements": r.replacements, "rel_residual": r.rel_residual, "solve_kernel_ms": r.kernel_ms,
+                "mpix_iter_s": N * r.iters / 1e3 / r.kernel_ms,
+                "solver_frac_of_measured_hbm": alg / (r.kernel_ms / 1000) / 1e9 / peaks["hbm_gbs"]})
+    dalpha = 2.0 * (alpha - gt) / N
+    for rep in range(2):
+        e0, e1 = ev()
+        e0.record(stream)
+        dimage, dgamma, lam, ra = st.adjoint(alpha, dalpha, rtol=1e-6, max_iters=5000, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    out.update({"adjoint_ms": e0.elapsed_time(e1), "adjoint_status": ra.status, "adjoint_iters": ra.iters,
+                "adjoint_rel_residual": ra.rel_residual,
+                "adjoint_solve_kernel_ms": ra.kernel_ms,
+                "adjoint_backprop_ms": e0.elapsed_time(e1) - ra.kernel_ms,
+                "dimage_finite": bool(torch.isfinite(dimage).all().item())})
+    return out
+
+
 def run_spmv(args, stream, peaks) -> dict:
     """Standalone SpMV passes at args.spmv_size^2 (inputs larger than L2, so
     no flush): gm_levin_apply on the FP16 store (iteration operator), on its
@@ -406,7 +473,7 @@ def run_spmv(args, stream, peaks) -> dict:
 
     S = args.spmv_size
     N = S * S
-    prob = make_problem(S, S, 0)
+    prob = cached_problem(S, S, 0)
     dev = torch.device("cuda", torch.cuda.current_device())
     img = torch.from_numpy(prob.image).to(dev)
     scr = torch.from_numpy(prob.scribbles).to(dev)
@@ -574,6 +641,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=64, help="batched-solve measurement: images (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--batch-only", action="store_true", help="profiling: only the batched solve")
+    ap.add_argument("--large-size", type=int, default=4096, help="large single solve + adjoint size (0 = skip)")
+    ap.add_argument("--large-only", action="store_true", help="profiling: only the large solve + adjoint")
     ap.add_argument("--replace-every", type=int, default=50)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="ring configuration: 0 auto, 3 shallow, 2 deep")
     args = ap.parse_args()
@@ -581,6 +650,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.large_only:
+        import torch
+
+        print(json.dumps({"large": run_large(args, torch.cuda.current_stream(), load_peaks())}), flush=True)
     elif args.batch_only:
         import torch
 

@@ -299,197 +299,131 @@ __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v)
     return old;
 }
 
+// Sum of p[lo .. hi-1] by one warp in a fixed order: lane l adds entries
+// l, l+32, l+64, ... in index order, then a fixed shuffle tree.  Every warp
+// that calls it on the same data gets the same bits (result in all lanes).
+// The loads of a chunk of 32 * 16 entries are all issued before any add, so a
+// grid's partials (<= 512 per component) cost one L2 round trip.
+__device__ __forceinline__ double warp_sum_range(const double* p, int lo, int hi)
+{
+    const int lane = threadIdx.x & 31;
+    constexpr int kU = 16;
+    double x = 0.0;
+    for (int base = lo; base < hi; base += 32 * kU) {
+        double v[kU];
+#pragma unroll
+        for (int j = 0; j < kU; ++j) {
+            const int i = base + lane + 32 * j;
+            v[j] = i < hi ? __ldcg(p + i) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < kU; ++j) x += v[j];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    return __shfl_sync(0xffffffffu, x, 0);
+}
+
+// Arrival half of the grid barrier, run by one thread: publish nothing more,
+// arrive with an acquire-release atomic (its release covers every write the
+// CTA made before the caller's __syncthreads), and spin on the generation
+// with acquire loads.  Returns 0 when the wait was abandoned.
+__device__ __forceinline__ int grid_arrive_wait(GridBarrier* gb, unsigned G, uint64_t limit_ns)
+{
+    const unsigned g = ld_acquire(&gb->gen);
+    const unsigned arrived = atom_add_acq_rel(&gb->count, 1u);
+    if (arrived == G - 1) {
+        gb->count = 0;
+        st_release(&gb->gen, g + 1);
+        return 1;
+    }
+    uint64_t t0 = 0;
+    unsigned spins = 0;
+    while (ld_acquire(&gb->gen) == g) {
+        ++spins;
+        if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) return 0;
+        if ((spins & 63u) == 0) {
+            const uint64_t now = globaltimer_ns();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > limit_ns) {
+                atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
+                atomicExch(&gb->where, 1);
+                return 0;
+            }
+        }
+    }
+    return 1;
+}
+
 // Grid barrier fused with a deterministic all-reduce of NV doubles per
 // thread.  On return every thread of every CTA holds the same bit-identical
 // grid totals in v.  parts is [NV][G] global scratch for this call (callers
 // alternate two copies so a fast CTA's next call cannot overwrite partials a
 // slow CTA is still reading).  scratch: >= 32 * NV + NV shared doubles.
-//
-// One warp does the grid part: lane 0 publishes the CTA sum and arrives with
-// an acquire-release atomic (its release covers every write the CTA made
-// before the first __syncthreads), spins on the generation with acquire
-// loads, and the warp then adds the G partials in a fixed order.  Two
-// __syncthreads per call in total.  Returns false when the barrier was
-// abandoned (limit reached or abort set by another CTA).
+// Components with index < NSEG are summed over CTAs lo .. hi-1 only (the
+// CTAs of one image in a batched solve), the others over the whole grid.
+// Warp 0 publishes the CTA sums and waits on the grid; after the release
+// each warp sums its components (k = warp, warp + nwarps, ...) with all of
+// its loads in flight at once.  Three __syncthreads per call.  Returns false
+// when the barrier was abandoned (limit reached or abort set by any CTA).
+template <int NV, int NSEG>
+__device__ __forceinline__ bool grid_allreduce_impl(GridBarrier* gb, double* parts, unsigned G, int lo, int hi,
+                                                    uint64_t limit_ns, double (&v)[NV], double* scratch)
+{
+    __shared__ int s_ok;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) scratch[wid * NV + k] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        double cs[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? scratch[lane * NV + k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            cs[k] = x;
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) parts[(size_t)k * G + blockIdx.x] = cs[k];
+            s_ok = grid_arrive_wait(gb, G, limit_ns);
+        }
+    }
+    __syncthreads();
+    const bool ok = s_ok != 0;
+    if (ok) {
+        for (int k = wid; k < NV; k += nw) {
+            const double t = k < NSEG ? warp_sum_range(parts + (size_t)k * G, lo, hi)
+                                      : warp_sum_range(parts + (size_t)k * G, 0, (int)G);
+            if (lane == 0) scratch[32 * NV + k] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = scratch[32 * NV + k];
+    return ok;
+}
+
 template <int NV>
 __device__ __forceinline__ bool grid_allreduce(GridBarrier* gb, double* parts, unsigned G, uint64_t limit_ns,
                                                double (&v)[NV], double* scratch)
 {
-    __shared__ int s_ok;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double x = v[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) scratch[wid * NV + k] = x;
-    }
-    __syncthreads();
-    if (wid == 0) {
-        double cs[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double x = lane < nw ? scratch[lane * NV + k] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            cs[k] = x;
-        }
-        int ok = 1;
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) parts[(size_t)k * G + blockIdx.x] = cs[k];
-            const unsigned g = ld_acquire(&gb->gen);
-            const unsigned arrived = atom_add_acq_rel(&gb->count, 1u);
-            if (arrived == G - 1) {
-                gb->count = 0;
-                st_release(&gb->gen, g + 1);
-            } else {
-                uint64_t t0 = 0;
-                unsigned spins = 0;
-                while (ld_acquire(&gb->gen) == g) {
-                    ++spins;
-                    if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) { ok = 0; break; }
-                    if ((spins & 63u) == 0) {
-                        const uint64_t now = globaltimer_ns();
-                        if (t0 == 0) t0 = now;
-                        else if (now - t0 > limit_ns) {
-                            atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
-                            atomicExch(&gb->where, 1);
-                            ok = 0;
-                            break;
-                        }
-                    }
-                }
-            }
-        }
-        __syncwarp();
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (ok) {
-            double a[NV], b[NV];
-#pragma unroll
-            for (int k = 0; k < NV; ++k) { a[k] = 0.0; b[k] = 0.0; }
-            int i = lane;
-            for (; i + 32 < (int)G; i += 64) {
-#pragma unroll
-                for (int k = 0; k < NV; ++k) {
-                    a[k] += __ldcg(parts + (size_t)k * G + i);
-                    b[k] += __ldcg(parts + (size_t)k * G + i + 32);
-                }
-            }
-            if (i < (int)G) {
-#pragma unroll
-                for (int k = 0; k < NV; ++k) a[k] += __ldcg(parts + (size_t)k * G + i);
-            }
-#pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                double x = a[k] + b[k];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-                if (lane == 0) scratch[32 * NV + k] = x;
-            }
-        }
-        if (lane == 0) s_ok = ok;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = scratch[32 * NV + k];
-    return s_ok != 0;
+    return grid_allreduce_impl<NV, 0>(gb, parts, G, 0, (int)G, limit_ns, v, scratch);
 }
 
-// Batched form of grid_allreduce: components 0 .. NV-2 are summed over the
-// CTAs lo .. hi-1 only (the CTAs of one image; lo == hi gives zeros) and
-// component NV-1 over the whole grid.  Same barrier, same fixed order, so
-// the CTAs of one image agree bit for bit.
+// Batched form: components 0 .. NV-2 over the CTAs lo .. hi-1 (one image;
+// lo == hi gives zeros), component NV-1 over the whole grid.
 template <int NV>
 __device__ __forceinline__ bool grid_allreduce_seg(GridBarrier* gb, double* parts, unsigned G, int lo, int hi,
                                                    uint64_t limit_ns, double (&v)[NV], double* scratch)
 {
-    __shared__ int s_ok;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double x = v[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) scratch[wid * NV + k] = x;
-    }
-    __syncthreads();
-    if (wid == 0) {
-        double cs[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double x = lane < nw ? scratch[lane * NV + k] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            cs[k] = x;
-        }
-        int ok = 1;
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) parts[(size_t)k * G + blockIdx.x] = cs[k];
-            const unsigned g = ld_acquire(&gb->gen);
-            const unsigned arrived = atom_add_acq_rel(&gb->count, 1u);
-            if (arrived == G - 1) {
-                gb->count = 0;
-                st_release(&gb->gen, g + 1);
-            } else {
-                uint64_t t0 = 0;
-                unsigned spins = 0;
-                while (ld_acquire(&gb->gen) == g) {
-                    ++spins;
-                    if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) { ok = 0; break; }
-                    if ((spins & 63u) == 0) {
-                        const uint64_t now = globaltimer_ns();
-                        if (t0 == 0) t0 = now;
-                        else if (now - t0 > limit_ns) {
-                            atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
-                            atomicExch(&gb->where, 1);
-                            ok = 0;
-                            break;
-                        }
-                    }
-                }
-            }
-        }
-        __syncwarp();
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (ok) {
-            double a[NV], b[NV];
-#pragma unroll
-            for (int k = 0; k < NV; ++k) { a[k] = 0.0; b[k] = 0.0; }
-            int i = lo + lane;
-            for (; i + 32 < hi; i += 64) {
-#pragma unroll
-                for (int k = 0; k < NV - 1; ++k) {
-                    a[k] += __ldcg(parts + (size_t)k * G + i);
-                    b[k] += __ldcg(parts + (size_t)k * G + i + 32);
-                }
-            }
-            if (i < hi) {
-#pragma unroll
-                for (int k = 0; k < NV - 1; ++k) a[k] += __ldcg(parts + (size_t)k * G + i);
-            }
-            const double* pl = parts + (size_t)(NV - 1) * G;
-            i = lane;
-            for (; i + 32 < (int)G; i += 64) {
-                a[NV - 1] += __ldcg(pl + i);
-                b[NV - 1] += __ldcg(pl + i + 32);
-            }
-            if (i < (int)G) a[NV - 1] += __ldcg(pl + i);
-#pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                double x = a[k] + b[k];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-                if (lane == 0) scratch[32 * NV + k] = x;
-            }
-        }
-        if (lane == 0) s_ok = ok;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = scratch[32 * NV + k];
-    return s_ok != 0;
+    return grid_allreduce_impl<NV, NV - 1>(gb, parts, G, lo, hi, limit_ns, v, scratch);
 }
 
 template <class T> struct Cvt;

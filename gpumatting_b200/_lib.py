@@ -24,7 +24,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "UNSUPPORTED", 4: "TIMEOUT"
                 6: "NOT_CONVERGED", 7: "NOMEM"}
 
 GM_PREC_FP32, GM_PREC_FP16, GM_PREC_BF16 = 0, 1, 2
-GM_SOLVER_CG, GM_SOLVER_GD, GM_SOLVER_JACOBI = 0, 1, 2
+GM_SOLVER_CG, GM_SOLVER_GD, GM_SOLVER_JACOBI, GM_SOLVER_PCG = 0, 1, 2, 3
 GM_IMAGE_RGB8, GM_IMAGE_RGBA32F = 0, 1
 GM_ASSEMBLY_FP64, GM_ASSEMBLY_REFERENCE = 0, 1
 

@@ -196,7 +196,7 @@ def compute_error(alpha, gt, W: int, H: int, stream=None) -> float:
 # Native: symmetric Levin store
 # ---------------------------------------------------------------------------
 PRECISIONS = {"fp32": L.GM_PREC_FP32, "fp16": L.GM_PREC_FP16, "bf16": L.GM_PREC_BF16}
-SOLVERS = {"cg": L.GM_SOLVER_CG, "gd": L.GM_SOLVER_GD, "jacobi": L.GM_SOLVER_JACOBI}
+SOLVERS = {"cg": L.GM_SOLVER_CG, "gd": L.GM_SOLVER_GD, "jacobi": L.GM_SOLVER_JACOBI, "pcg": L.GM_SOLVER_PCG}
 
 
 def _image_desc(image) -> L.GmImage:

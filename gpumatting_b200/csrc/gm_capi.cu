@@ -71,6 +71,10 @@ extern "C" int gm_banded_solve(BandedMatrix L, int W, float* alpha, int pad, con
     if (prm) p = *prm; else gm_default_params(&p);
     cudaStream_t st = (cudaStream_t)stream;
     if (!alpha || !b || !L.a || L.rows <= 0) { gm_set_error_msg("gm_banded_solve: bad arguments"); return GM_ERR_INVALID; }
+    if (p.solver == GM_SOLVER_PCG) {
+        gm_set_error_msg("GM_SOLVER_PCG runs on the symmetric Levin store (gm_levin_solve), not on 25 bands");
+        return GM_ERR_UNSUPPORTED;
+    }
     std::vector<int> offs;
     GM_TRY(read_offsets(L, offs, st));
     int Wd = 0;

@@ -359,7 +359,7 @@ __device__ __forceinline__ int grid_arrive_wait(GridBarrier* gb, unsigned G, uin
 // thread.  On return every thread of every CTA holds the same bit-identical
 // grid totals in v.  parts is [NV][G] global scratch for this call (callers
 // alternate two copies so a fast CTA's next call cannot overwrite partials a
-// slow CTA is still reading).  scratch: >= 32 * NV + NV shared doubles.
+// slow CTA is still reading).  scratch: >= (warps + 1) * NV shared doubles.
 // Components with index < NSEG are summed over CTAs lo .. hi-1 only (the
 // CTAs of one image in a batched solve), the others over the whole grid.
 // Warp 0 publishes the CTA sums and waits on the grid; after the release
@@ -401,12 +401,12 @@ __device__ __forceinline__ bool grid_allreduce_impl(GridBarrier* gb, double* par
         for (int k = wid; k < NV; k += nw) {
             const double t = k < NSEG ? warp_sum_range(parts + (size_t)k * G, lo, hi)
                                       : warp_sum_range(parts + (size_t)k * G, 0, (int)G);
-            if (lane == 0) scratch[32 * NV + k] = t;
+            if (lane == 0) scratch[nw * NV + k] = t;
         }
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = scratch[32 * NV + k];
+    for (int k = 0; k < NV; ++k) v[k] = scratch[nw * NV + k];
     return ok;
 }
 

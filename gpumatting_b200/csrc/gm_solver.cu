@@ -246,7 +246,7 @@ __device__ __forceinline__ void load_rows(V (&X)[6][6], const V* ring, int r0, i
     }
 }
 
-template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, int KIND>
+template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, int KIND, bool PCG = false>
 __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& geo, unsigned char* smem, int u0,
                                           int v0, int v1, const KState& s, double (&part)[kNPart], Pipe& pp)
 {
@@ -257,17 +257,18 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     const int nband = nsteps - 2;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
-    unsigned char* vring = smem + L.vring_off;
-    unsigned char* bring = smem + L.bring_off;
+    unsigned char* vring = smem + K.vbase;
+    unsigned char* bring = smem + K.bbase;
     volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + kRedBytes);
     constexpr bool kSymBand = (KIND == KIND_KRYLOV ? OPLO : OPHI) != OP_REF25;
 
     if (warp == kConsumers) {
         // ------------------------------ producer ------------------------------
         if (lane != 0) return;
-        const CUtensorMap* vm[4] = {nullptr, nullptr, nullptr, nullptr};
+        const CUtensorMap* vm[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
         if (KIND == KIND_KRYLOV) {
             vm[0] = &A.m_r[s.c]; vm[1] = &A.m_q[s.c]; vm[2] = &A.m_p[s.c]; vm[3] = &A.m_xacc[s.xsel];
+            if (PCG) vm[4] = &A.m_xlo;  // the diagonal, for z = r / d
         } else if (KIND == KIND_REPLACE) {
             vm[0] = MIXED ? &A.m_base[s.xsel] : nullptr; vm[1] = &A.m_xacc[s.xsel]; vm[2] = &A.m_p[s.c];
             vm[3] = &A.m_b;
@@ -276,7 +277,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
         }
         const CUtensorMap* bm = KIND == KIND_KRYLOV ? &A.m_wlo : &A.m_whi;
         const CUtensorMap* xm = KIND == KIND_KRYLOV ? &A.m_xlo : &A.m_xhi;
-        const uint32_t vbytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2] + K.vbytes[3];
+        const uint32_t vbytes = K.vbytes[0] + K.vbytes[1] + K.vbytes[2] + K.vbytes[3] + (vm[4] ? K.vbytes[4] : 0);
         fence_proxy_async();
         // Issue in the consumers' order: super-step j takes vector rows j and
         // j+1, then band rows up to (its last step) - 2.  Matching the order
@@ -292,8 +293,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             unsigned char* dst = vring + vs * K.vslot;
             mbar_arrive_expect_tx(&full[vs], vbytes);
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (K.vbytes[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, v0 - 2 + t, &full[vs]);
+            for (int i = 0; i < 5; ++i)
+                if (K.vbytes[i] && vm[i]) tma_load_2d(dst + K.voff[i], vm[i], u0 - 8, v0 - 2 + t, &full[vs]);
             vs = ring_next(vs, K.Rv);
             return true;
         };
@@ -344,6 +345,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * 4 * kWarpCols;  // r or b, own columns
     const int P = A.P;
     constexpr int Rb = K.Rb;
+    constexpr bool pcg = PCG && OPLO == OP_SYMD && KIND == KIND_KRYLOV;  // Jacobi-preconditioned CG
 
     int vs = 0;    // vector slot of the next step
     int bsn = 0;   // band slot of the next band step to wait for
@@ -369,7 +371,9 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             const float* vq = reinterpret_cast<const float*>(vsp + K.voff[1]);
             const float* vp = reinterpret_cast<const float*>(vsp + K.voff[2]);
             const float* vx = reinterpret_cast<const float*>(vsp + K.voff[3]);
-            auto combine = [&](int cc, float2& rn, float2& pv) {
+            const float* vd = reinterpret_cast<const float*>(vsp + K.voff[4]);
+            // r' = r - alpha q; z' = r' / d (Jacobi PCG) or r'; p' = z' + beta p
+            auto combine = [&](int cc, float2& rn, float2& zn, float2& pv) {
                 const float2 rv = ld2(vr, cc);
                 pv = ld2(vp, cc);
                 if (s.skipR) {
@@ -378,17 +382,25 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                     const float2 qv = ld2(vq, cc);
                     rn = make_float2(fmaf(-s.af, qv.x, rv.x), fmaf(-s.af, qv.y, rv.y));
                 }
-                return s.beta_zero ? rn : make_float2(fmaf(s.bf, pv.x, rn.x), fmaf(s.bf, pv.y, rn.y));
+                if constexpr (pcg) {
+                    // d = 0 only outside the image (TMA zero fill), where r = 0 too
+                    const float2 dv = ld2(vd, cc);
+                    zn = make_float2(dv.x > 0.f ? __fdividef(rn.x, dv.x) : 0.f,
+                                     dv.y > 0.f ? __fdividef(rn.y, dv.y) : 0.f);
+                } else {
+                    zn = rn;
+                }
+                return s.beta_zero ? zn : make_float2(fmaf(s.bf, pv.x, zn.x), fmaf(s.bf, pv.y, zn.y));
             };
-            float2 rn, pv;
-            const float2 pn = combine(c, rn, pv);
+            float2 rn, zn, pv;
+            const float2 pn = combine(c, rn, zn, pv);
             *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lc0 + 2) = pn;
             if (has_x) {
-                float2 rx, px;
-                *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lcx) = combine(cx, rx, px);
+                float2 rx, zx, px;
+                *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lcx) = combine(cx, rx, zx, px);
             }
             if (own_row) {
-                *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = rn;
+                *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = zn;
                 if (in1) {
                     *reinterpret_cast<float2*>(A.r[s.c ^ 1] + gi) = rn;
                     *reinterpret_cast<float2*>(A.p[s.c ^ 1] + gi) = pn;
@@ -397,12 +409,14 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         *reinterpret_cast<float2*>(A.xacc[s.xsel] + gi) =
                             make_float2(fmaf(s.af, pv.x, xv.x), fmaf(s.af, pv.y, xv.y));
                     }
-                    part[0] += (double)fmaf(rn.x, rn.x, rn.y * rn.y);
+                    part[0] += (double)fmaf(rn.x, zn.x, rn.y * zn.y);
+                    if constexpr (pcg) part[4] += (double)fmaf(rn.x, rn.x, rn.y * rn.y);
                 } else if (in0) {
                     A.r[s.c ^ 1][gi] = rn.x;
                     A.p[s.c ^ 1][gi] = pn.x;
                     if (!s.skipR) A.xacc[s.xsel][gi] = fmaf(s.af, pv.x, vx[c]);
-                    part[0] += (double)rn.x * (double)rn.x;
+                    part[0] += (double)rn.x * (double)zn.x;
+                    if constexpr (pcg) part[4] += (double)rn.x * (double)rn.x;
                 }
             }
         } else if (KIND == KIND_REPLACE) {
@@ -522,18 +536,33 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         ref25_apply<float, 0>(q0.x, q0.y, d0, d1, X, bA[0], c);
                         if (second) ref25_apply<float, 1>(q1.x, q1.y, d0, d1, X, bB[0], c);
                     }
+                    // own ring: z (= r for plain CG) of the output rows
                     const float2 rn0 = *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0);
                     const float2 rn1 = *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0);
+                    // q M^-1 q: the diagonal of output rows v, v+1 sits in their band rows
+                    float2 w0 = make_float2(1.f, 1.f), w1 = make_float2(1.f, 1.f);
+                    if constexpr (pcg) {
+                        {
+                            const float2 d0 = ld2(reinterpret_cast<const float*>(bA[0] + K.xoff), c);
+                            w0 = make_float2(d0.x > 0.f ? __fdividef(1.f, d0.x) : 0.f,
+                                             d0.y > 0.f ? __fdividef(1.f, d0.y) : 0.f);
+                            if (second) {
+                                const float2 d1 = ld2(reinterpret_cast<const float*>(bB[0] + K.xoff), c);
+                                w1 = make_float2(d1.x > 0.f ? __fdividef(1.f, d1.x) : 0.f,
+                                                 d1.y > 0.f ? __fdividef(1.f, d1.y) : 0.f);
+                            }
+                        }
+                    }
                     if (in1) {
                         *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go) = q0;
                         float spq = fmaf(X[2][2], q0.x, X[2][3] * q0.y);
                         float srq = fmaf(rn0.x, q0.x, rn0.y * q0.y);
-                        float sqq = fmaf(q0.x, q0.x, q0.y * q0.y);
+                        float sqq = fmaf(q0.x * w0.x, q0.x, q0.y * w0.y * q0.y);
                         if (second) {
                             *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go + P) = q1;
                             part[1] += (double)fmaf(X[3][2], q1.x, X[3][3] * q1.y);
                             part[2] += (double)fmaf(rn1.x, q1.x, rn1.y * q1.y);
-                            part[3] += (double)fmaf(q1.x, q1.x, q1.y * q1.y);
+                            part[3] += (double)fmaf(q1.x * w1.x, q1.x, q1.y * w1.y * q1.y);
                         }
                         part[1] += (double)spq;
                         part[2] += (double)srq;
@@ -542,12 +571,12 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         A.q[s.c ^ 1][go] = q0.x;
                         part[1] += (double)X[2][2] * (double)q0.x;
                         part[2] += (double)rn0.x * (double)q0.x;
-                        part[3] += (double)q0.x * (double)q0.x;
+                        part[3] += (double)q0.x * w0.x * (double)q0.x;
                         if (second) {
                             A.q[s.c ^ 1][go + P] = q1.x;
                             part[1] += (double)X[3][2] * (double)q1.x;
                             part[2] += (double)rn1.x * (double)q1.x;
-                            part[3] += (double)q1.x * (double)q1.x;
+                            part[3] += (double)q1.x * w1.x * (double)q1.x;
                         }
                     }
                 } else if (KIND == KIND_REPLACE) {
@@ -705,9 +734,10 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     int kind = jac ? KIND_JACOBI : KIND_REPLACE;
     KState s;
     s.af = 0.f; s.bf = 0.f; s.ad = 0.0; s.skipR = true; s.beta_zero = true; s.c = 0; s.xsel = 0;
-    double rr_prev = 0.0, bb = -1.0, rr_true = 0.0, rel = 0.0;
+    double rr_prev = 0.0, bb = -1.0, rr_true = 0.0, rel = 0.0, be_pred = 0.0;
     bool final_rep = false, restart_due = false;
     const bool gd = A.solver == GM_SOLVER_GD;
+    const bool pcg_mode = A.solver == GM_SOLVER_PCG;
     if (jac && A.max_iters <= 0) {
         kind = KIND_REPLACE;
         final_rep = true;
@@ -717,9 +747,12 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     bool done = BATCH && img < 0;
 
     while (ok) {
-        double part[kNPart] = {0.0, 0.0, 0.0, 0.0};
+        double part[kNPart] = {};
         if (active && !done) {
-            if (kind == KIND_KRYLOV)
+            if (kind == KIND_KRYLOV && pcg_mode)
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV, OPLO == OP_SYMD>(A, geo, smem, u0, v0, v1, s,
+                                                                                    part, pp);
+            else if (kind == KIND_KRYLOV)
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, geo, smem, u0, v0, v1, s, part, pp);
             else if (kind == KIND_REPLACE)
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_REPLACE>(A, geo, smem, u0, v0, v1, s, part, pp);
@@ -727,17 +760,31 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, geo, smem, u0, v0, v1, s, part, pp);
         }
         if constexpr (BATCH) {
-            double v5[kNPart + 1] = {part[0], part[1], part[2], part[3], done ? 0.0 : 1.0};
-            ok = grid_allreduce_seg<kNPart + 1>(A.gb, A.partials + (size_t)parity * G * (kNPart + 1), G, lo, hi,
-                                                A.limit_ns, v5, red);
-            if (!ok) break;
+            // per-image sums + "CTAs still working" over the grid (last component)
+            double* parts = A.partials + (size_t)parity * G * (kNPart + 1);
+            double running;
+            if (pcg_mode) {
+                double v6[kNPart + 1] = {part[0], part[1], part[2], part[3], part[4], done ? 0.0 : 1.0};
+                ok = grid_allreduce_seg<kNPart + 1>(A.gb, parts, G, lo, hi, A.limit_ns, v6, red);
 #pragma unroll
-            for (int k = 0; k < kNPart; ++k) part[k] = v5[k];
+                for (int k = 0; k < kNPart; ++k) part[k] = v6[k];
+                running = v6[kNPart];
+            } else {
+                double v5[kNPart] = {part[0], part[1], part[2], part[3], done ? 0.0 : 1.0};
+                ok = grid_allreduce_seg<kNPart>(A.gb, parts, G, lo, hi, A.limit_ns, v5, red);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) part[k] = v5[k];
+                running = v5[4];
+            }
+            if (!ok) break;
             parity ^= 1;
-            if (!(v5[kNPart] > 0.0)) break;  // no CTA worked in this sweep: every image is done
+            if (!(running > 0.0)) break;  // no CTA worked in this sweep: every image is done
             if (done) continue;
         } else {
-            ok = grid_allreduce<kNPart>(A.gb, A.partials + (size_t)parity * G * kNPart, G, A.limit_ns, part, red);
+            // four sums for CG, GD and Jacobi; PCG adds r.r
+            double* parts = A.partials + (size_t)parity * G * kNPart;
+            if (pcg_mode) ok = grid_allreduce<kNPart>(A.gb, parts, G, A.limit_ns, part, red);
+            else ok = grid_allreduce<4>(A.gb, parts, G, A.limit_ns, *reinterpret_cast<double(*)[4]>(part), red);
             if (!ok) break;
             parity ^= 1;
         }
@@ -746,6 +793,9 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
         if (kind == KIND_KRYLOV) {
             s.c ^= 1;
             ++it;
+            // CG: rr = r.r, rq = r.q, qq = q.q.  Jacobi PCG: rr = r.z, rq = q.z,
+            // qq = q.M^-1 q (z = M^-1 r, M = diag(d)); tot[4] = r.r.  The same
+            // recurrence then predicts the next r.r (CG) or r.z (PCG).
             const double rr = tot[0], pq = tot[1], rq = tot[2], qq = tot[3];
             if (isfinite(rr) && !(rr > 1e-32 * bb)) {
                 // residual at the end of FP64 precision (exactly 0 on tiny
@@ -766,11 +816,14 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
             double rr_pred = rr - 2.0 * al * rq + al * al * qq;
             if (rr_pred < 0.0) rr_pred = 0.0;
             rr_prev = rr;
+            be_pred = rr_pred / rr;
             s.ad = al;
             s.af = (float)al;
             const bool rep_due = A.replace_every > 0 && it % A.replace_every == 0;
             restart_due = A.restart > 0 && it % A.restart == 0;
-            const bool tol_hit = A.rtol > 0.0 && rr_pred <= A.rtol * A.rtol * bb;
+            // PCG tests the residual of this sweep (r.r is exact, one iteration
+            // behind the CG prediction)
+            const bool tol_hit = A.rtol > 0.0 && (A.solver == GM_SOLVER_PCG ? tot[4] : rr_pred) <= A.rtol * A.rtol * bb;
             if (rep_due || restart_due || tol_hit || it >= A.max_iters) {
                 kind = KIND_REPLACE;
                 final_rep = it >= A.max_iters;
@@ -800,7 +853,9 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
                 }
             }
             const bool bz = restart_due || gd || !(rr_prev > 0.0);
-            const double be = bz ? 0.0 : rr_true / rr_prev;
+            // after a replacement CG rescales with the true residual; PCG keeps
+            // the predicted r.z ratio (the replacement sweep has no diagonal)
+            const double be = bz ? 0.0 : (A.solver == GM_SOLVER_PCG ? be_pred : rr_true / rr_prev);
             s.bf = (float)be;
             s.beta_zero = bz;
             s.skipR = true;

@@ -20,8 +20,9 @@ constexpr int kBox = kStrip + 16;                // TMA box width: strip + 8 col
 constexpr int kRingCols = kWarpCols + 4;         // private operand ring: warp columns + 2 each side
 constexpr int kRvMax = 16;                       // vector ring slots
 constexpr int kRbMax = 16;                       // band ring slots
-constexpr int kNPart = 4;                        // FP64 partial sums per CTA per sweep
-constexpr int kRedBytes = (32 + 1) * (kNPart + 1) * 8;  // reduction scratch: warp sums + grid totals
+constexpr int kNPart = 5;                        // FP64 partial sums per CTA per sweep
+// reduction scratch: per-warp sums + grid totals of up to kNPart + 1 values
+constexpr int kRedBytes = (kThreads / 32 + 1) * (kNPart + 1) * 8;
 
 // Shared-memory carve of one sweep kind.  Everything here is a compile-time
 // function of the operator types, so the hot loop indexes rings with
@@ -31,8 +32,10 @@ struct KindLayout {
     int Rv, Rb;     // ring slots
     int vslot;      // bytes per vector slot
     int bslot;      // bytes per band slot
-    int voff[4];    // offsets of the vector rows inside a vector slot
-    int vbytes[4];  // TMA bytes of each vector row (0 = unused)
+    int vbase;      // offset of the vector ring in the ring area
+    int bbase;      // offset of the band ring in the ring area
+    int voff[5];    // offsets of the vector rows inside a vector slot
+    int vbytes[5];  // TMA bytes of each vector row (0 = unused)
     int planes;     // band planes loaded per row
     int pstride;    // bytes between planes inside a band slot (= kBox * elem)
     int xoff;       // offset of the extra plane row (diagonal or gamma), -1 none
@@ -41,18 +44,22 @@ struct KindLayout {
 
 __host__ __device__ constexpr int a128(int x) { return (x + 127) & ~127; }
 
-// Vector rows per step: Krylov r, q, p, x increment; replacement base (FP64,
-// mixed only), x increment, p, b; Jacobi x, -, -, b.
+// Vector rows per step: Krylov r, q, p, x increment, and the diagonal d for
+// the Jacobi preconditioner (symmetric store; loaded only by PCG solves);
+// replacement base (FP64, mixed only), x increment, p, b; Jacobi x, -, -, b.
 __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize, bool mixed, int Rv, int Rb)
 {
     KindLayout K{};
     const int vb4 = kBox * 4;
-    int vb[4] = {0, 0, 0, 0};
-    if (kind == KIND_KRYLOV) { vb[0] = vb4; vb[1] = vb4; vb[2] = vb4; vb[3] = vb4; }
+    int vb[5] = {0, 0, 0, 0, 0};
+    if (kind == KIND_KRYLOV) {
+        vb[0] = vb4; vb[1] = vb4; vb[2] = vb4; vb[3] = vb4;
+        vb[4] = op == OP_SYMD ? vb4 : 0;
+    }
     else if (kind == KIND_REPLACE) { vb[0] = mixed ? 2 * vb4 : 0; vb[1] = vb4; vb[2] = vb4; vb[3] = vb4; }
     else { vb[0] = vb4; vb[3] = vb4; }
     int off = 0;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 5; ++i) {
         K.voff[i] = off;
         K.vbytes[i] = vb[i];
         off += a128(vb[i]);
@@ -68,6 +75,8 @@ __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize
     K.D = Rv - 1;
     K.Rv = Rv;
     K.Rb = Rb;
+    K.vbase = 0;
+    K.bbase = a128(Rv * K.vslot);
     return K;
 }
 
@@ -90,8 +99,10 @@ __host__ __device__ constexpr int rings_b(int kind, int oplo, int cfg)
 // solution is kept in FP64 (mixed), FP32 otherwise.
 __host__ __device__ constexpr int ring_esize(bool mixed) { return mixed ? 8 : 4; }
 
+// The vector and band rings of a sweep share one area whose split depends on
+// the sweep kind (a sweep starts with both rings drained).
 struct Layout {
-    int vring_off, bring_off, pring_off, rring_off, full_off, empty_off, red_off, total;
+    int ring_bytes, pring_off, rring_off, full_off, empty_off, red_off, total;
     KindLayout k[NKIND];
 };
 
@@ -103,14 +114,10 @@ __host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int oph
     for (int k = 0; k < NKIND; ++k)
         L.k[k] = kind_layout(k, k == KIND_KRYLOV ? oplo : ophi, k == KIND_KRYLOV ? esize_lo : 4, mixed,
                              rings_v(k, oplo, cfg), rings_b(k, oplo, cfg));
-    int vcap = 0, bcap = 0;
-    for (int k = 0; k < NKIND; ++k) {
-        vcap = imax(vcap, L.k[k].Rv * L.k[k].vslot);
-        bcap = imax(bcap, L.k[k].Rb * L.k[k].bslot);
-    }
-    L.vring_off = 0;
-    L.bring_off = a128(vcap);
-    L.pring_off = L.bring_off + a128(bcap);
+    int cap = 0;
+    for (int k = 0; k < NKIND; ++k) cap = imax(cap, L.k[k].bbase + L.k[k].Rb * L.k[k].bslot);
+    L.ring_bytes = a128(cap);
+    L.pring_off = L.ring_bytes;
     L.rring_off = L.pring_off + a128(kConsumers * 8 * kRingCols * ring_esize(mixed));
     L.full_off = L.rring_off + a128(kConsumers * 4 * kWarpCols * 4);
     L.empty_off = L.full_off + a128((kRvMax + kRbMax) * 8);

@@ -160,7 +160,10 @@ int gm_compute_error(double* mse_host, const float* alpha, const float* gt, int 
 /* ------------------------------------------------------------------ */
 
 enum { GM_PREC_FP32 = 0, GM_PREC_FP16 = 1, GM_PREC_BF16 = 2 };
-enum { GM_SOLVER_CG = 0, GM_SOLVER_GD = 1, GM_SOLVER_JACOBI = 2 };
+/* GM_SOLVER_PCG: CG preconditioned with the operator's diagonal (Jacobi);
+ * symmetric store only (gm_levin_solve*, batches).  No counterpart in the
+ * reference, whose cgSolve is unpreconditioned. */
+enum { GM_SOLVER_CG = 0, GM_SOLVER_GD = 1, GM_SOLVER_JACOBI = 2, GM_SOLVER_PCG = 3 };
 enum { GM_IMAGE_RGB8 = 0, GM_IMAGE_RGBA32F = 1 };
 /* Assembly arithmetic: FP64 throughout (rounded once), or the reference's
  * float/double mix (bit-identical to hostLevinLaplacian). */

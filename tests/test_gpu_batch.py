@@ -137,3 +137,17 @@ def test_batch_timeout_status_and_recovery():
         a.fill_(0.5)
     res = b.solve(alphas, "cg", rtol=1e-6, ctas_per_sm=3)
     assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res)
+
+
+def test_batch_pcg_reaches_rtol_per_image(orc):
+    torch = torch_cuda()
+    b, probs = _batch("fp16")
+    alphas = [torch.full((H, W), 0.5, device="cuda") for W, H in SIZES]
+    res = b.solve(alphas, "pcg", rtol=1e-6, max_iters=5000)
+    alphas_cg = [torch.full((H, W), 0.5, device="cuda") for W, H in SIZES]
+    res_cg = b.solve(alphas_cg, "cg", rtol=1e-6, max_iters=5000)
+    for k, (W, H) in enumerate(SIZES):
+        assert res[k].status == 0 and res[k].rel_residual <= 1e-6, (k, res[k])
+        w32, g, bb = _view_planes(b, k, W, H)
+        assert _relres(orc, w32, g, bb, alphas[k].double().cpu().numpy(), W, H) <= 1.05e-6, k
+    assert sum(r.iters for r in res) < sum(r.iters for r in res_cg)

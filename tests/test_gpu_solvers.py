@@ -7,6 +7,8 @@ import pytest
 
 from gpu_util import bands25_f32, oracle_problem, torch_cuda
 
+from gpumatting_b200.synth import make_problem
+
 pytestmark = pytest.mark.gpu
 TOL = 1e-4  # max-abs alpha tolerance against the FP64 oracle
 
@@ -210,3 +212,76 @@ def test_bad_arguments():
     alpha = torch.zeros((16, 16), device="cuda")
     with pytest.raises(L.GmError):
         st.solve(alpha, "cg", max_iters=-1)
+
+
+def _pcg64(op, diag, b, x0, rtol, maxit=20000):
+    """FP64 Jacobi-preconditioned CG (M = diag of the operator)."""
+    x = x0.copy()
+    r = b - op.apply(x)
+    z = r / diag
+    p = z.copy()
+    rz = r @ z
+    bn = np.linalg.norm(b)
+    for it in range(maxit):
+        if np.linalg.norm(r) <= rtol * bn:
+            return x, it
+        q = op.apply(p)
+        al = rz / (p @ q)
+        x += al * p
+        r -= al * q
+        z = r / diag
+        rz2 = r @ z
+        p = z + (rz2 / rz) * p
+        rz = rz2
+    return x, maxit
+
+
+@pytest.mark.parametrize("prec", ["fp16", "bf16", "fp32"])
+def test_levin_pcg_to_rtol(orc, prec):
+    """Jacobi-preconditioned mixed CG: true FP64 residual at rtol, about as
+    many iterations as FP64 Jacobi PCG, and fewer than plain CG."""
+    torch = torch_cuda()
+    W, H = 160, 120
+    api, st, p, w, g, b = _store(orc, W, H, prec)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    res = st.solve(alpha, "pcg", rtol=1e-6, max_iters=5000)
+    assert res.status == 0 and res.rel_residual <= 1e-6, res
+    x = alpha.double().cpu().numpy().ravel()
+    assert _true_relres(orc, st, g, b, x) <= 1.05e-6
+    op = orc.Operator(W=W, H=H, w=w, gamma=g)
+    diag = orc.sym_to_bands64(w, g, W, H)[12]
+    _, it64 = _pcg64(op, diag, b, np.full(W * H, 0.5), 1e-6)
+    assert res.iters <= 1.3 * it64 + 20, (res.iters, it64)
+    alpha.fill_(0.5)
+    res_cg = st.solve(alpha, "cg", rtol=1e-6, max_iters=5000)
+    assert res.iters <= 0.85 * res_cg.iters, (res.iters, res_cg.iters)
+
+
+def test_levin_pcg_accurate_and_deterministic(orc):
+    torch = torch_cuda()
+    W, H = 96, 64
+    api, st, p, w, g, b = _store(orc, W, H, "fp16", seed=3)
+    outs = []
+    for _ in range(2):
+        alpha = torch.full((H, W), 0.5, device="cuda")
+        res = st.solve(alpha, "pcg", rtol=1e-10, max_iters=20000)
+        assert res.status == 0 and res.rel_residual <= 1e-10, res
+        outs.append(alpha.cpu().numpy())
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    w32 = st.planes("w32")[:, :, :W].reshape(12, -1).double().cpu().numpy()
+    xs, _, _ = orc.Operator(W=W, H=H, w=w32, gamma=g).cg(b, np.full(W * H, 0.5), rtol=1e-13, maxit=100000)
+    assert np.abs(outs[0].astype(np.float64).ravel() - xs).max() <= TOL
+
+
+def test_pcg_rejected_on_25_band_store():
+    torch = torch_cuda()
+    from gpumatting_b200 import _lib as L
+    from gpumatting_b200 import api
+
+    p = make_problem(40, 30, 1)
+    a, b = api.levin_bands25(torch.from_numpy(p.image).cuda(), torch.from_numpy(p.scribbles).cuda(), eps=p.eps)
+    Lm = api.DeviceBandedMatrix(a, torch.tensor(api.levin_band_offsets(40), device="cuda"), 40 * 30)
+    x = api.PaddedVector(40 * 30, api.levin_pad(40))
+    with pytest.raises(L.GmError) as e:
+        api.banded_solve(Lm, x, b, W=40, solver="pcg", rtol=1e-6)
+    assert e.value.status == L.GM_ERR_UNSUPPORTED

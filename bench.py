@@ -367,9 +367,30 @@ def run_ours(args):
                     "d2h_bytes_per_step": N * 4, "ms_per_step": 1000 * te_max / args.steps},
             "gpu_launches": 3 * args.steps,  # per step: levin_sym_kernel, levin_diag_kernel, solver_kernel
             "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_pcg:
+        # the same step with Jacobi-preconditioned mixed CG, to the same true rel-res
+        def step_pcg():
+            store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
+            alpha.copy_(a0_d, non_blocking=True)
+            return store.solve(alpha, "pcg", **params)
+
+        for _ in range(2):
+            step_pcg()
+        ms_p, res_p = timed(step_pcg, args.steps)
+        assert all(r.status == 0 and (args.fixed_iters or r.rel_residual <= 1e-6) for r in res_p), res_p
+        it_p = sum(r.iters for r in res_p)
+        line["pcg"] = {"solver": "Jacobi-preconditioned mixed CG (FP16 store, FP64 replacement every 50)",
+                       "ms_per_step": sum(ms_p) / args.steps, "iters_per_solve": it_p / args.steps,
+                       "replacements_per_solve": sum(r.replacements for r in res_p) / args.steps,
+                       "rel_residual_max": max(r.rel_residual for r in res_p),
+                       "mpix_iter_s": N * it_p / 1e6 / (sum(ms_p) / 1000),
+                       "solver_kernel_ms": sum(r.kernel_ms for r in res_p) / args.steps}
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_fp32"] = run_plain(args, prob, img_d, scr_d, flush, stream)
         line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
+        if "pcg" in line:
+            line["plain_fp32"]["speedup_mixed_pcg_vs_plain"] = (line["plain_fp32"]["ms_per_solve"]
+                                                                / line["pcg"]["ms_per_step"])
     if args.batch_count > 0:
         line["batch"] = run_batch(args, stream, world, rank)
     if rank == 0 and world == 1 and args.large_size > 0:
@@ -447,18 +468,26 @@ def run_large(args, stream, peaks) -> dict:
                 "replacements": r.replacements, "rel_residual": r.rel_residual, "solve_kernel_ms": r.kernel_ms,
                 "mpix_iter_s": N * r.iters / 1e3 / r.kernel_ms,
                 "solver_frac_of_measured_hbm": alg / (r.kernel_ms / 1000) / 1e9 / peaks["hbm_gbs"]})
-    dalpha = 2.0 * (alpha - gt) / N
     for rep in range(2):
-        e0, e1 = ev()
-        e0.record(stream)
-        dimage, dgamma, lam, ra = st.adjoint(alpha, dalpha, rtol=1e-6, max_iters=5000, stream=stream)
-        e1.record(stream)
+        alpha.fill_(0.5)
+        rp = st.solve(alpha, "pcg", rtol=1e-6, max_iters=5000, stream=stream)
         torch.cuda.synchronize()
-    out.update({"adjoint_ms": e0.elapsed_time(e1), "adjoint_status": ra.status, "adjoint_iters": ra.iters,
-                "adjoint_rel_residual": ra.rel_residual,
-                "adjoint_solve_kernel_ms": ra.kernel_ms,
-                "adjoint_backprop_ms": e0.elapsed_time(e1) - ra.kernel_ms,
-                "dimage_finite": bool(torch.isfinite(dimage).all().item())})
+    out.update({"pcg_status": rp.status, "pcg_iters": rp.iters, "pcg_rel_residual": rp.rel_residual,
+                "pcg_solve_kernel_ms": rp.kernel_ms})
+    dalpha = 2.0 * (alpha - gt) / N
+    for solver in ("cg", "pcg"):
+        for rep in range(2):
+            e0, e1 = ev()
+            e0.record(stream)
+            dimage, dgamma, lam, ra = st.adjoint(alpha, dalpha, solver=solver, rtol=1e-6, max_iters=5000,
+                                                 stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        key = "adjoint" if solver == "cg" else "adjoint_pcg"
+        out.update({f"{key}_ms": e0.elapsed_time(e1), f"{key}_status": ra.status, f"{key}_iters": ra.iters,
+                    f"{key}_rel_residual": ra.rel_residual, f"{key}_solve_kernel_ms": ra.kernel_ms,
+                    f"{key}_backprop_ms": e0.elapsed_time(e1) - ra.kernel_ms,
+                    f"{key}_dimage_finite": bool(torch.isfinite(dimage).all().item())})
     return out
 
 
@@ -552,6 +581,18 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
         if i >= 2:
             ms.append(e0.elapsed_time(e1))
     assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res), [r.status for r in res]
+    ms_pcg = []
+    for i in range(1 + args.batch_steps):
+        for a in alphas:
+            a.fill_(0.5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res_p = batch.solve(alphas, "pcg", rtol=1e-6, max_iters=5000, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= 1:
+            ms_pcg.append(e0.elapsed_time(e1))
+    assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res_p), [r.status for r in res_p]
     its = [r.iters for r in res]
     batch_ms = allreduce_max(statistics.mean(ms), world)
     work = allreduce_sum(sum(W * H * i for (W, H), i in zip(sizes, its)), world)
@@ -560,7 +601,10 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
            "sizes": "W, H uniform in [256, 1024], seed 0; size-balanced bins of whole images per GPU",
            "batch_ms": batch_ms, "batch_mpix_iter_s": work / 1e3 / batch_ms,
            "iters_min_mean_max": [min(its), statistics.mean(its), max(its)],
-           "launch": "1 cooperative launch per GPU from a CUDA graph", "tuned_shape": shape, "tune_s": t_tune}
+           "launch": "1 cooperative launch per GPU from a CUDA graph", "tuned_shape": shape, "tune_s": t_tune,
+           "batch_pcg_ms": allreduce_max(statistics.mean(ms_pcg), world),
+           "pcg_iters_min_mean_max": [min(r.iters for r in res_p), statistics.mean(r.iters for r in res_p),
+                                      max(r.iters for r in res_p)]}
     if world > 1:
         return out
     # sequential plain FP32 solves of the same images
@@ -582,7 +626,8 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
         seq_its.append(r.iters)
         del a, b, Lm, x
     out.update({"sequential_plain_fp32_ms": seq_ms, "sequential_iters_mean": statistics.mean(seq_its),
-                "speedup_vs_sequential_plain": seq_ms / batch_ms})
+                "speedup_vs_sequential_plain": seq_ms / batch_ms,
+                "pcg_speedup_vs_sequential_plain": seq_ms / out["batch_pcg_ms"]})
     return out
 
 
@@ -629,6 +674,7 @@ def main():
     ap.add_argument("--H", type=int, default=1080)
     ap.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-pcg", action="store_true", help="skip the Jacobi-preconditioned comparison")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

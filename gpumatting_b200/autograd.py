@@ -18,7 +18,7 @@ from . import api
 class LevinMatte(torch.autograd.Function):
     @staticmethod
     def forward(ctx, image, gamma, s, eps: float, precision: str, rtol: float, max_iters: int,
-                adjoint_rtol: float):
+                adjoint_rtol: float, solver: str):
         if image.dim() != 3 or image.shape[2] != 3 or image.dtype != torch.float32 or not image.is_cuda:
             raise ValueError("image must be a CUDA float32 tensor of shape (H, W, 3)")
         H, W, _ = image.shape
@@ -30,11 +30,12 @@ class LevinMatte(torch.autograd.Function):
         sv = s.detach().to(torch.float32).contiguous()
         store = api.LevinStore(W, H, precision).assemble(im4, gamma_map=g, s_map=sv, eps=eps)
         alpha = torch.full((H, W), 0.5, dtype=torch.float32, device=image.device)
-        res = store.solve(alpha, "cg", rtol=rtol, max_iters=max_iters)
+        res = store.solve(alpha, solver, rtol=rtol, max_iters=max_iters)
         ctx.store = store
         ctx.solve = res
         ctx.adjoint_rtol = adjoint_rtol
         ctx.max_iters = max_iters
+        ctx.solver = solver
         ctx.save_for_backward(alpha)
         return alpha
 
@@ -42,14 +43,15 @@ class LevinMatte(torch.autograd.Function):
     def backward(ctx, grad_alpha):
         (alpha,) = ctx.saved_tensors
         dimage, dgamma, _, res = ctx.store.adjoint(alpha, grad_alpha.detach().to(torch.float32).contiguous(),
-                                                   rtol=ctx.adjoint_rtol, max_iters=ctx.max_iters)
+                                                   solver=ctx.solver, rtol=ctx.adjoint_rtol, max_iters=ctx.max_iters)
         ctx.adjoint_solve = res
-        return dimage[..., :3].contiguous(), dgamma, None, None, None, None, None, None
+        return dimage[..., :3].contiguous(), dgamma, None, None, None, None, None, None, None
 
 
 def levin_matte(image, gamma, s, eps: float = 1e-5, precision: str = "fp16", rtol: float = 1e-6,
-                max_iters: int = 5000, adjoint_rtol: float | None = None):
+                max_iters: int = 5000, adjoint_rtol: float | None = None, solver: str = "cg"):
     """Differentiable matte: alpha (H, W) from image (H, W, 3) in [0, 1],
-    per-pixel scribble weights gamma and targets s (both (H, W))."""
+    per-pixel scribble weights gamma and targets s (both (H, W)).  solver:
+    "cg" or "pcg" (Jacobi-preconditioned) for both the solve and the adjoint."""
     return LevinMatte.apply(image, gamma, s, eps, precision, rtol, max_iters,
-                            rtol if adjoint_rtol is None else adjoint_rtol)
+                            rtol if adjoint_rtol is None else adjoint_rtol, solver)

@@ -44,6 +44,11 @@ class GmScribbles(C.Structure):
                 ("gamma_map", C.c_void_p), ("s_map", C.c_void_p)]
 
 
+class GmPnm(C.Structure):
+    _fields_ = [("w", C.c_int), ("h", C.c_int), ("channels", C.c_int), ("maxval", C.c_int),
+                ("data", C.POINTER(C.c_ubyte))]
+
+
 class GmLevinStore(C.Structure):
     _fields_ = [("W", C.c_int), ("H", C.c_int), ("pitch", C.c_int), ("precision", C.c_int), ("w", C.c_void_p),
                 ("w32", C.c_void_p), ("gamma", C.c_void_p), ("b", C.c_void_p), ("d", C.c_void_p),
@@ -111,6 +116,12 @@ SIGNATURES = {
     "gm_batch_solve": (_i, [_vp, C.POINTER(C.c_void_p), C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo), _vp]),
     "gm_batch_info": (_i, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                            C.POINTER(C.c_int)]),
+    "gm_pnm_read": (_i, [C.c_char_p, C.POINTER(GmPnm)]),
+    "gm_pnm_free": (None, [C.POINTER(GmPnm)]),
+    "gm_pgm_write": (_i, [C.c_char_p, _i, _i, _vp, C.c_char_p, _i]),
+    "gm_rgb8_to_float4": (_i, [_vp, _vp, _i, _i, _vp]),
+    "gm_alpha_to_gray8": (_i, [_vp, _vp, _i, _vp]),
+    "gm_bands_dump": (_i, [C.c_char_p, BandedMatrix, _i]),
     "gm_levin_apply": (_i, [C.POINTER(GmLevinStore), _vp, _i, _vp, _i, _i, _vp]),
     "gm_levin_solve_rhs": (_i, [C.POINTER(GmLevinStore), _vp, _vp, C.POINTER(GmSolveParams),
                                 C.POINTER(GmSolveInfo), _vp]),

@@ -439,3 +439,55 @@ def banded_solve(Lm: DeviceBandedMatrix, alpha: PaddedVector, b, W: int = 0, sol
     if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
         L.check(rc)
     return SolveResult.from_info(info)
+
+
+# ---------------------------------------------------------------------------
+# Data formats either side of the solve (ppm.h, main.cu:334-355)
+# ---------------------------------------------------------------------------
+def read_pnm(path: str):
+    """PNM file -> (uint8 array (H, W) or (H, W, 3), maxval) (ppm.h:32-127, :178-278)."""
+    img = L.GmPnm()
+    L.check(L.load().gm_pnm_read(str(path).encode(), C.byref(img)))
+    shape = (img.h, img.w) if img.channels == 1 else (img.h, img.w, 3)
+    maxval = img.maxval
+    try:
+        data = np.ctypeslib.as_array(img.data, shape=(img.w * img.h * img.channels,)).copy()
+    finally:
+        L.load().gm_pnm_free(C.byref(img))
+    return data.reshape(shape), maxval
+
+
+def write_pgm(path: str, gray: np.ndarray, comment: str | None = None, binary: bool = True):
+    """8-bit graymap file, the reference's pgmwrite bytes (ppm.h:345-414)."""
+    g = np.ascontiguousarray(gray, dtype=np.uint8)
+    h, w = g.shape
+    L.check(L.load().gm_pgm_write(str(path).encode(), w, h, g.ctypes.data, None if comment is None else
+                                  comment.encode(), int(binary)))
+
+
+def rgb8_to_float4(rgb, maxval: int = 255, stream=None):
+    """Device RGB bytes (H, W, 3) -> (H, W, 4) float32, (r, g, b, 1) / maxval (ppm.h:309-333)."""
+    torch = _torch()
+    H, W, _ = rgb.shape
+    out = torch.empty((H, W, 4), dtype=torch.float32, device=rgb.device)
+    L.check(L.load().gm_rgb8_to_float4(out.data_ptr(), rgb.contiguous().data_ptr(), H * W, maxval, _stream(stream)))
+    return out
+
+
+def alpha_to_gray8(alpha, stream=None):
+    """Device alpha -> uint8 matte, clamped and truncated as pgmwrite_float (ppm.h:430-451)."""
+    torch = _torch()
+    out = torch.empty(alpha.shape, dtype=torch.uint8, device=alpha.device)
+    L.check(L.load().gm_alpha_to_gray8(out.data_ptr(), alpha.contiguous().data_ptr(), alpha.numel(), _stream(stream)))
+    return out
+
+
+def write_alpha_pgm(path: str, alpha, comment: str | None = None, binary: bool = True, stream=None):
+    """The reference's alpha.pgm: quantised on the device, written on the host."""
+    g = alpha_to_gray8(alpha, stream).cpu().numpy()
+    write_pgm(path, g, comment, binary)
+
+
+def dump_bands(path: str, Lm: DeviceBandedMatrix):
+    """A.bin: nbands x rows float32, band-major (main.cu:334-355)."""
+    L.check(L.load().gm_bands_dump(str(path).encode(), Lm.struct, 1))

@@ -293,6 +293,36 @@ int gm_levin_adjoint(const gm_levin_store* st, const gm_image* im, const gm_scri
                      gm_solve_info* info, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* Data formats either side of the solve                               */
+/* ------------------------------------------------------------------ */
+
+/* A PNM image as read from a file: host bytes, w*h*channels, row-major. */
+typedef struct gm_pnm_s {
+    int w, h;
+    int channels;         /* 1 (P5/P2 graymap) or 3 (P6/P3 pixmap)        */
+    int maxval;
+    unsigned char* data;  /* host memory owned by the struct: gm_pnm_free */
+} gm_pnm;
+
+/* ppm.h:32-127 pgmread and :178-278 ppmread: binary or ASCII, header lines
+ * as the reference reads them; pixmaps with maxval outside 0..255 are
+ * rejected as the reference rejects them.  Host only. */
+int gm_pnm_read(const char* path, gm_pnm* img);
+void gm_pnm_free(gm_pnm* img);
+/* ppm.h:345-414 pgmwrite: "P5"/"P2", optional "# comment", maxval 255; the
+ * same bytes as the reference writes.  data: host w*h bytes. */
+int gm_pgm_write(const char* path, int w, int h, const unsigned char* data, const char* comment, int binary);
+/* ppm.h:309-333 ppmread_float4's normalisation on the device: RGB bytes to
+ * (r, g, b, 1) / maxval.  dst 16-byte aligned. */
+int gm_rgb8_to_float4(gm_float4* dst, const unsigned char* src, int n, int maxval, void* stream);
+/* ppm.h:430-451 pgmwrite_float's quantisation on the device: 0 below 0, 255
+ * above 1, else (unsigned char)(255 * alpha). */
+int gm_alpha_to_gray8(unsigned char* dst, const float* alpha, int n, void* stream);
+/* main.cu:334-355 dump: the A.bin file, nbands x rows floats, band-major.
+ * on_device: L.a is device memory (copied band by band). */
+int gm_bands_dump(const char* path, BandedMatrix L, int on_device);
+
+/* ------------------------------------------------------------------ */
 /* Batched solves: many images of different sizes in one persistent   */
 /* launch (no counterpart in the reference, which solves one image).   */
 /* ------------------------------------------------------------------ */

@@ -87,8 +87,48 @@ def reflib():
         R.ref_jacobi_host.argtypes = [_f, _f, C.c_size_t, _i, C.c_int, C.c_int, _f, C.c_size_t,
                                       C.c_int, C.c_float]
         R.ref_jacobi_host.restype = C.c_int
+        R.ref_pgmread.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        R.ref_pgmread.restype = C.c_void_p
+        R.ref_ppmread.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        R.ref_ppmread.restype = C.c_void_p
+        R.ref_ppmread_float4.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        R.ref_ppmread_float4.restype = C.c_void_p
+        R.ref_pgmwrite_float.argtypes = [C.c_char_p, C.c_int, C.c_int, _f, C.c_char_p, C.c_int]
+        R.ref_pgmwrite_float.restype = C.c_int
+        R.ref_free.argtypes = [C.c_void_p]
         _ref = R
     return _ref
+
+
+def ref_read_pnm(path: str, color: bool):
+    """The reference's ppmread / pgmread (valid files only): (bytes array, maxval or None)."""
+    R = reflib()
+    w, h, mv = C.c_int(0), C.c_int(0), C.c_int(0)
+    if color:
+        ptr = R.ref_ppmread(str(path).encode(), C.byref(w), C.byref(h), C.byref(mv))
+        n, shape = w.value * h.value * 3, (h.value, w.value, 3)
+    else:
+        ptr = R.ref_pgmread(str(path).encode(), C.byref(w), C.byref(h))
+        n, shape = w.value * h.value, (h.value, w.value)
+    data = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_ubyte)), shape=(n,)).copy().reshape(shape)
+    R.ref_free(ptr)
+    return data, (mv.value if color else None)
+
+
+def ref_ppmread_float4(path: str) -> np.ndarray:
+    R = reflib()
+    w, h = C.c_int(0), C.c_int(0)
+    ptr = R.ref_ppmread_float4(str(path).encode(), C.byref(w), C.byref(h))
+    out = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(w.value * h.value * 4,)).copy()
+    R.ref_free(ptr)
+    return out.reshape(h.value, w.value, 4)
+
+
+def ref_pgmwrite_float(path: str, alpha: np.ndarray, comment: str | None, binary: bool) -> int:
+    a = np.ascontiguousarray(alpha, np.float32)
+    h, w = a.shape
+    return reflib().ref_pgmwrite_float(str(path).encode(), w, h, P(a, _f),
+                                       None if comment is None else comment.encode(), int(binary))
 
 
 def P(a: np.ndarray, t):

@@ -7,6 +7,10 @@
  * restatement and to generate the golden fixtures in tests/golden/.
  *
  * Wrapped functions:
+ *   pgmread, ppmread    ppm.h:32-127, :178-278 (valid files only: the
+ *                       reference exits on some malformed ones)
+ *   ppmread_float4      ppm.h:309-333
+ *   pgmwrite_float      ppm.h:430-451
  *   hostLevinLaplacian  Matting.cu:39-219
  *   gaussSeidel_host    Solve.cpp:3-33
  *   jacobi_host         Solve.cpp:35-85
@@ -16,6 +20,7 @@
  */
 #include "Matting.cu"
 #include "Solve.h"
+#include "ppm.h"
 
 extern "C" {
 
@@ -63,5 +68,18 @@ int ref_jacobi_host(float* x, float* a, size_t apitch, int* bands, int nbands,
     jacobi_host(x, A, b, iterations, xpad, omega);
     return 0;
 }
+
+
+unsigned char* ref_pgmread(char* filename, int* w, int* h) { return pgmread(filename, w, h); }
+unsigned char* ref_ppmread(char* filename, int* w, int* h, int* maxval) { return ppmread(filename, w, h, maxval); }
+float* ref_ppmread_float4(char* filename, int* w, int* h)
+{
+    return reinterpret_cast<float*>(ppmread_float4(0, filename, w, h));
+}
+int ref_pgmwrite_float(char* filename, int w, int h, float* data, const char* comment, int binsave)
+{
+    return pgmwrite_float(filename, w, h, data, comment, binsave);
+}
+void ref_free(void* p) { free(p); }
 
 }

@@ -653,8 +653,18 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     release_bands_to(nband);
 }
 
+// Resident CTAs per SM the register budget is sized for: 3 for the 2-byte
+// symmetric stores with shallow rings (their shared memory allows 3), 1 (no
+// register cap) for the other configurations, which shared memory limits to 2.
+template <class TLo, int OPLO, int CFG>
+constexpr int solver_min_blocks()
+{
+    return (OPLO == OP_SYMD && sizeof(TLo) == 2 && CFG == 0) ? 3 : 1;
+}
+
 template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, bool BATCH>
-__global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant__ SolverArgs A)
+__global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
+    solver_kernel(const __grid_constant__ SolverArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;
@@ -666,22 +676,18 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     // This CTA's unit: a 192-column strip of a row segment of one image.
     int img = -1, u0 = 0, v0 = 0, v1 = 0, lo = 0, hi = 0;
     UnitGeo geo;
+    int u0b = 0, v0b = 0, v1b = 0;  // second piece (batched units only)
     if constexpr (BATCH) {
         geo.W = 0; geo.arow0 = 0; geo.apitch = 0; geo.aout = nullptr; geo.ain = nullptr;
-        const int b = blockIdx.x;
-        for (int k = 0; k < A.nimg; ++k) {
-            const BatchImage I = A.imgs[k];
-            if (b >= I.c0 && b < I.c0 + I.units) {
-                img = k;
-                const int unit = b - I.c0;
-                const int st = unit % I.nstrips, sg = unit / I.nstrips;
-                u0 = st * kStrip;
-                v0 = I.y0 + (int)((long long)I.H * sg / I.nseg);
-                v1 = I.y0 + (int)((long long)I.H * (sg + 1) / I.nseg);
-                lo = I.c0;
-                hi = I.c0 + I.units;
-                geo.W = I.W; geo.arow0 = I.y0; geo.apitch = I.W; geo.aout = I.alpha; geo.ain = I.alpha;
-            }
+        const BatchUnit U = A.units[blockIdx.x];
+        if (U.img >= 0 && U.img < A.nimg) {
+            const BatchImage I = A.imgs[U.img];
+            img = U.img;
+            u0 = U.u0[0]; v0 = U.v0[0]; v1 = U.v1[0];
+            u0b = U.u0[1]; v0b = U.v0[1]; v1b = U.v1[1];
+            lo = I.c0;
+            hi = I.c0 + I.units;
+            geo.W = I.W; geo.arow0 = I.y0; geo.apitch = I.W; geo.aout = I.alpha; geo.ain = I.alpha;
         }
     } else {
         const int unit = blockIdx.x;
@@ -693,7 +699,6 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
         }
         geo.W = A.W; geo.arow0 = 0; geo.apitch = A.alpha_pitch; geo.aout = A.alpha_out; geo.ain = A.alpha_in;
     }
-    const bool active = v1 > v0;
 
     if (tid == 0) {
         for (int i = 0; i < kRvMax + kRbMax; ++i) {
@@ -709,10 +714,12 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
     const bool jac = A.solver == GM_SOLVER_JACOBI;
     // Import the initial guess and the right-hand side; zero the first
     // search direction.
-    if (active) {
-        for (int v = v0; v < v1; ++v)
+#pragma unroll 1
+    for (int piece = 0; piece < (BATCH ? 2 : 1); ++piece) {
+        const int pu0 = piece ? u0b : u0, pv0 = piece ? v0b : v0, pv1 = piece ? v1b : v1;
+        for (int v = pv0; v < pv1; ++v)
             for (int cl = tid; cl < kStrip; cl += blockDim.x) {
-                const int u = u0 + cl;
+                const int u = pu0 + cl;
                 if (u >= geo.W) continue;
                 const size_t i = (size_t)v * A.P + u;
                 const float a0 = geo.ain[(size_t)(v - geo.arow0) * geo.apitch + u];
@@ -748,16 +755,19 @@ __global__ void __launch_bounds__(kThreads) solver_kernel(const __grid_constant_
 
     while (ok) {
         double part[kNPart] = {};
-        if (active && !done) {
+#pragma unroll 1
+        for (int piece = 0; piece < (BATCH ? 2 : 1); ++piece) {
+            const int pu0 = piece ? u0b : u0, pv0 = piece ? v0b : v0, pv1 = piece ? v1b : v1;
+            if (!(pv1 > pv0) || done) continue;
             if (kind == KIND_KRYLOV && pcg_mode)
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV, OPLO == OP_SYMD>(A, geo, smem, u0, v0, v1, s,
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV, OPLO == OP_SYMD>(A, geo, smem, pu0, pv0, pv1, s,
                                                                                     part, pp);
             else if (kind == KIND_KRYLOV)
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, geo, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, geo, smem, pu0, pv0, pv1, s, part, pp);
             else if (kind == KIND_REPLACE)
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_REPLACE>(A, geo, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_REPLACE>(A, geo, smem, pu0, pv0, pv1, s, part, pp);
             else
-                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, geo, smem, u0, v0, v1, s, part, pp);
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_JACOBI>(A, geo, smem, pu0, pv0, pv1, s, part, pp);
         }
         if constexpr (BATCH) {
             // per-image sums + "CTAs still working" over the grid (last component)

@@ -148,6 +148,17 @@ struct BatchImage {
     float* alpha;             // [H][W] device: initial guess in, solution out
 };
 
+// A CTA's share of a batched solve: rows of up to two strips of one image
+// (a run of strip-rows that may continue from the bottom of one strip into
+// the top of the next), so the CTAs of an image get equal row counts to
+// within one row.  Rows are canvas rows; v1 <= v0 marks an absent piece.
+struct BatchUnit {
+    int img;                  // -1: no work
+    int u0[2];                // strip start column
+    int v0[2], v1[2];         // canvas rows [v0, v1)
+    int pad_;
+};
+
 // Where a CTA's unit lives: image width for masking, and where its solution
 // rows go (row vr of the canvas is row vr - arow0 of aout).
 struct UnitGeo {
@@ -191,6 +202,7 @@ struct SolverArgs {
     int inject;              // 1: first grid barrier expects one extra arrival
     // batched solves (BATCH kernels only)
     const BatchImage* imgs;
+    const BatchUnit* units;  // [grid]
     int nimg;
     SolverOut* outs;         // [nimg]
 };

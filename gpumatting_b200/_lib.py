@@ -122,6 +122,7 @@ SIGNATURES = {
     "gm_rgb8_to_float4": (_i, [_vp, _vp, _i, _i, _vp]),
     "gm_alpha_to_gray8": (_i, [_vp, _vp, _i, _vp]),
     "gm_bands_dump": (_i, [C.c_char_p, BandedMatrix, _i]),
+    "gm_levin_restrict": (_i, [C.POINTER(GmLevinStore), C.POINTER(GmScribbles), _vp]),
     "gm_levin_apply": (_i, [C.POINTER(GmLevinStore), _vp, _i, _vp, _i, _i, _vp]),
     "gm_levin_solve_rhs": (_i, [C.POINTER(GmLevinStore), _vp, _vp, C.POINTER(GmSolveParams),
                                 C.POINTER(GmSolveInfo), _vp]),

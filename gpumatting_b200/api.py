@@ -260,6 +260,14 @@ class LevinStore:
         self._inputs = (image, scribbles, eps, gamma_value, gamma_map, s_map)
         return self
 
+    def restrict(self, scribbles=None, gamma_map=None, s_map=None, stream=None):
+        """Hard-constrain the known pixels (scribbled, or gamma_map > 0) to their
+        targets and eliminate them: the store then holds the system on the
+        unknown pixels (gm_levin_restrict)."""
+        sc = _scrib_desc(scribbles, 1.0, gamma_map, s_map)
+        L.check(L.load().gm_levin_restrict(C.byref(self.s), C.byref(sc), _stream(stream)))
+        return self
+
     def planes(self, which: str = "w32"):
         """Views of the store's device planes as torch tensors (H, pitch)."""
         torch = _torch()

@@ -502,6 +502,80 @@ __global__ void __launch_bounds__(TW * TH) levin_adjoint_kernel(ImgView im, Scri
     }
 }
 
+// ---------------------------------------------------------------------------
+// Restriction to the unknown pixels (hard constraints)
+// ---------------------------------------------------------------------------
+// Pixels with a scribble (or a positive gamma_map weight) are known: their
+// value is fixed at the target s.  The store becomes the system on the
+// unknown pixels with the known ones eliminated: for an unknown pixel i and a
+// known neighbour j, w_ij (x_i - s_j) moves to the diagonal (gamma_i += w_ij)
+// and the right-hand side (b_i += w_ij s_j); known rows become x_i = s_i;
+// every coupling that touches a known pixel is removed.  Pass 1 gathers the
+// new gamma and b per pixel (reads planes only), pass 2 zeroes the removed
+// couplings, then the diagonal planes are recomputed.
+
+__device__ __forceinline__ bool known_at(const ScribView& s, int u, int v, float& target)
+{
+    float gam, bv;
+    const bool has = scribble(s, u, v, gam, bv);
+    target = scribble_target(s, u, v);
+    return has && gam > 0.f;
+}
+
+__global__ void levin_restrict_gather_kernel(ScribView sc, const float* __restrict__ w32, float* gamma, float* b,
+                                             int W, int H, int pitch, size_t plane)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W) return;
+    const size_t i = (size_t)v * pitch + u;
+    float si;
+    if (known_at(sc, u, v, si)) {
+        gamma[i] = 1.f;
+        b[i] = si;
+        return;
+    }
+    double g = gamma[i], bb = b[i];
+#pragma unroll
+    for (int k = 1; k <= 12; ++k) {
+        const int dv = (k + 2) / 5, du = k - 5 * dv;
+        const int uf = u + du, vf = v + dv;  // upper partner: coupling stored at i
+        float sj;
+        if (uf >= 0 && uf < W && vf < H && known_at(sc, uf, vf, sj)) {
+            const double w = w32[(size_t)(k - 1) * plane + i];
+            g += w;
+            bb += w * (double)sj;
+        }
+        const int ul = u - du, vl = v - dv;  // lower partner: coupling stored at the partner
+        if (ul >= 0 && ul < W && vl >= 0 && known_at(sc, ul, vl, sj)) {
+            const double w = w32[(size_t)(k - 1) * plane + (size_t)vl * pitch + ul];
+            g += w;
+            bb += w * (double)sj;
+        }
+    }
+    gamma[i] = __double2float_rn(g);
+    b[i] = __double2float_rn(bb);
+}
+
+template <class T>
+__global__ void levin_restrict_cut_kernel(ScribView sc, T* w, float* w32, int W, int H, int pitch, size_t plane)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= W) return;
+    const size_t i = (size_t)v * pitch + u;
+    float t;
+    const bool ki = known_at(sc, u, v, t);
+#pragma unroll
+    for (int k = 1; k <= 12; ++k) {
+        const int dv = (k + 2) / 5, du = k - 5 * dv;
+        const int uf = u + du, vf = v + dv;
+        const bool kj = uf >= 0 && uf < W && vf < H && known_at(sc, uf, vf, t);
+        if (ki || kj) {
+            w[(size_t)(k - 1) * plane + i] = from_double<T>(0.0);
+            w32[(size_t)(k - 1) * plane + i] = 0.f;
+        }
+    }
+}
+
 }  // namespace gm
 
 using namespace gm;
@@ -652,6 +726,44 @@ int gm_levin_adjoint_grads(const gm_image* im, const gm_scribbles* sc, double ep
     o.dgamma = dgamma;
     dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH);
     levin_adjoint_kernel<<<grid, TW * TH, 0, stream>>>(iv, sv, eps, W, H, lam, alpha, o);
+    GM_CUDA_TRY(cudaGetLastError());
+    return GM_OK;
+}
+
+extern "C" int gm_levin_restrict(gm_levin_store* st, const gm_scribbles* sc, void* stream)
+{
+    if (!st || !st->w || !st->w32 || !st->gamma || !st->b || !st->d || !st->d32 || !sc) {
+        gm_set_error_msg("gm_levin_restrict: bad arguments");
+        return GM_ERR_INVALID;
+    }
+    if (!sc->map && !sc->gamma_map) { gm_set_error_msg("gm_levin_restrict: no known pixels given"); return GM_ERR_INVALID; }
+    GM_TRY(gm_check_device(nullptr));
+    ScribView sv;
+    memset(&sv, 0, sizeof(sv));
+    sv.W = st->W;
+    sv.map = sc->map;
+    sv.map_pitch = sc->map_pitch ? sc->map_pitch : (size_t)st->W;
+    sv.gamma_value = 1.f;  // only "known or not" matters here
+    sv.gamma_map = sc->gamma_map;
+    sv.s_map = sc->s_map;
+    const int W = st->W, H = st->H, P = st->pitch;
+    const size_t plane = st->plane_stride ? st->plane_stride : (size_t)H * P;
+    cudaStream_t s = (cudaStream_t)stream;
+    dim3 g((W + 127) / 128, H);
+    levin_restrict_gather_kernel<<<g, 128, 0, s>>>(sv, st->w32, st->gamma, st->b, W, H, P, plane);
+    if (st->precision == GM_PREC_FP16)
+        levin_restrict_cut_kernel<__half><<<g, 128, 0, s>>>(sv, (__half*)st->w, st->w32, W, H, P, plane);
+    else if (st->precision == GM_PREC_BF16)
+        levin_restrict_cut_kernel<__nv_bfloat16><<<g, 128, 0, s>>>(sv, (__nv_bfloat16*)st->w, st->w32, W, H, P, plane);
+    else
+        levin_restrict_cut_kernel<float><<<g, 128, 0, s>>>(sv, (float*)st->w, st->w32, W, H, P, plane);
+    if (st->precision == GM_PREC_FP16)
+        levin_diag_kernel<__half><<<g, 128, 0, s>>>((const __half*)st->w, st->w32, st->gamma, st->d, st->d32, W, H, P, plane);
+    else if (st->precision == GM_PREC_BF16)
+        levin_diag_kernel<__nv_bfloat16><<<g, 128, 0, s>>>((const __nv_bfloat16*)st->w, st->w32, st->gamma, st->d,
+                                                           st->d32, W, H, P, plane);
+    else
+        levin_diag_kernel<float><<<g, 128, 0, s>>>((const float*)st->w, st->w32, st->gamma, st->d, st->d32, W, H, P, plane);
     GM_CUDA_TRY(cudaGetLastError());
     return GM_OK;
 }

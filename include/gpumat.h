@@ -220,6 +220,16 @@ int gm_levin_store_free(gm_levin_store* st);
 int gm_levin_assemble(gm_levin_store* st, const gm_image* im, const gm_scribbles* sc,
                       double eps, BandedMatrix* bands25, float* b25, void* stream);
 
+/* Restrict an assembled store to the unknown pixels (hard constraints): the
+ * pixels `sc` marks as known (map 0/255, or gamma_map > 0 with targets s_map)
+ * are fixed at their targets and eliminated.  Unknown rows keep their full
+ * diagonal, their couplings to known pixels move to the right-hand side
+ * (b_i += w_ij s_j) and are removed; known rows become x_i = s_i, decoupled
+ * from the rest (an initial guess equal to s there keeps them exact; from any
+ * other guess they converge with the solve).  Levin's trimap restriction, left commented out in the
+ * reference (matlab/getLevinLap.m:20, :24, :33-35); no C counterpart. */
+int gm_levin_restrict(gm_levin_store* st, const gm_scribbles* sc, void* stream);
+
 /* Reference-layout assembly only (25 bands FP32 + b), with either
  * arithmetic.  a, b: device; a has 25 planes of apitch floats. */
 int gm_levin_assemble_bands25(float* a, size_t apitch, float* b, const gm_image* im,

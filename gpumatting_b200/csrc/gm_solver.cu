@@ -209,6 +209,14 @@ struct KState {
     int xsel;        // solution buffers read this sweep
 };
 
+// The solver state of one image (every CTA of the image holds the same copy
+// in registers); batched solves publish it when CTAs are re-dealt.
+struct ImgState {
+    KState s;
+    int status, it, nrep, kind, final_rep, restart_due;
+    double rr_prev, bb, rr_true, rel, be_pred;
+};
+
 // Per-thread pipeline state that lives across sweeps: one bit per ring slot.
 struct Pipe {
     uint32_t full_v, full_b;    // consumers: parity of the next full-barrier phase
@@ -653,6 +661,72 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     release_bands_to(nband);
 }
 
+// The unit of CTA b after a re-deal (run by one warp; lane 0 writes out[]):
+// the strip-row partition of the host (batch_partition, rmul 1) over the
+// images that have not finished.  out = {img, u0, v0, v1, u0b, v0b, v1b, lo,
+// hi}; img = -1 when b gets no work.  Every CTA computes the same partition.
+__device__ __noinline__ void batch_redeal(const SolverArgs& A, int b, int G, int* out)
+{
+    const int lane = threadIdx.x & 31;
+    auto running = [&](int k) { return __ldcg(A.img_done + k) == 0; };
+    int maxT = 0;
+    for (int k = lane; k < A.nimg; k += 32)
+        if (running(k)) {
+            const BatchImage I = A.imgs[k];
+            maxT = max(maxT, ((I.W + kStrip - 1) / kStrip) * I.H);
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxT = max(maxT, __shfl_xor_sync(0xffffffffu, maxT, o));
+    int R = max(maxT, 1);
+    if (maxT > 0) {
+        int rlo = 1, rhi = maxT;
+        while (rlo < rhi) {
+            const int mid = rlo + (rhi - rlo) / 2;
+            long long c = 0;
+            for (int k = lane; k < A.nimg; k += 32)
+                if (running(k)) {
+                    const BatchImage I = A.imgs[k];
+                    const int sk = (I.W + kStrip - 1) / kStrip, T = sk * I.H;
+                    c += max(sk, (T + mid - 1) / mid);
+                }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (c <= G) rhi = mid; else rlo = mid + 1;
+        }
+        R = rlo;
+    }
+    if (lane != 0) return;
+    int res[9] = {-1, 0, 0, 0, 0, 0, 0, 0, 0};
+    int c0 = 0;
+    for (int k = 0; k < A.nimg && maxT > 0; ++k) {
+        if (!running(k)) continue;
+        const BatchImage I = A.imgs[k];
+        const int sk = (I.W + kStrip - 1) / kStrip, H = I.H;
+        const long long T = (long long)sk * H;
+        const long long nk = (T + R - 1) / R;
+        const int n = (int)(nk > sk ? nk : (long long)sk);
+        if (b >= c0 && b < c0 + n) {
+            const int u = b - c0;
+            const long long t0 = T * u / n, t1 = T * (u + 1) / n;
+            const int sa = (int)(t0 / H), ra = (int)(t0 % H), sb = (int)((t1 - 1) / H);
+            res[0] = k;
+            res[1] = sa * kStrip;
+            res[2] = I.y0 + ra;
+            res[3] = I.y0 + (sb == sa ? (int)((t1 - 1) % H) + 1 : H);
+            if (sb != sa) {
+                res[4] = sb * kStrip;
+                res[5] = I.y0;
+                res[6] = I.y0 + (int)((t1 - 1) % H) + 1;
+            }
+            res[7] = c0;
+            res[8] = c0 + n;
+            break;
+        }
+        c0 += n;
+    }
+    for (int q = 0; q < 9; ++q) out[q] = res[q];
+}
+
 // Resident CTAs per SM the register budget is sized for: 3 for the 2-byte
 // symmetric stores with shallow rings (their shared memory allows 3), 1 (no
 // register cap) for the other configurations, which shared memory limits to 2.
@@ -752,8 +826,51 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
     // Batched solves: a CTA whose image has converged (or that has no image)
     // keeps joining the grid barrier with no work until every image is done.
     bool done = BATCH && img < 0;
+    // Batched solves re-deal the CTAs when images finish (the grid-wide count
+    // of CTAs that worked in a sweep dropped): the images still running
+    // publish their state, and after a barrier every CTA computes the same
+    // strip-row partition over them and takes up its new image's state.
+    bool redeal = false;
+    double prev_running = -1.0;
 
     while (ok) {
+        if constexpr (BATCH) {
+            if (redeal) {
+                redeal = false;
+                ImgState* tab = reinterpret_cast<ImgState*>(A.states);
+                if (img >= 0 && !done && (int)blockIdx.x == lo && tid == 0) {
+                    ImgState t;
+                    t.s = s; t.status = status; t.it = it; t.nrep = nrep; t.kind = kind;
+                    t.final_rep = final_rep; t.restart_due = restart_due;
+                    t.rr_prev = rr_prev; t.bb = bb; t.rr_true = rr_true; t.rel = rel; t.be_pred = be_pred;
+                    tab[img] = t;
+                }
+                ok = grid_sync(A.gb, G, A.limit_ns);
+                if (!ok) break;
+                __shared__ int s_unit[9];  // img, u0, v0, v1, u0b, v0b, v1b, lo, hi
+                if (tid < 32) batch_redeal(A, (int)blockIdx.x, (int)G, s_unit);
+                __syncthreads();
+                img = s_unit[0];
+                u0 = s_unit[1]; v0 = s_unit[2]; v1 = s_unit[3];
+                u0b = s_unit[4]; v0b = s_unit[5]; v1b = s_unit[6];
+                lo = s_unit[7]; hi = s_unit[8];
+                __syncthreads();
+                done = img < 0;
+                if (!done) {
+                    const BatchImage I = A.imgs[img];
+                    geo.W = I.W; geo.arow0 = I.y0; geo.apitch = I.W; geo.aout = I.alpha; geo.ain = I.alpha;
+                    // written by another CTA before the barrier: read past L1
+                    ImgState tv;
+                    const int* src = reinterpret_cast<const int*>(tab + img);
+                    int* dst = reinterpret_cast<int*>(&tv);
+#pragma unroll
+                    for (int q = 0; q < (int)(sizeof(ImgState) / sizeof(int)); ++q) dst[q] = __ldcg(src + q);
+                    s = tv.s; status = tv.status; it = tv.it; nrep = tv.nrep; kind = tv.kind;
+                    final_rep = tv.final_rep != 0; restart_due = tv.restart_due != 0;
+                    rr_prev = tv.rr_prev; bb = tv.bb; rr_true = tv.rr_true; rel = tv.rel; be_pred = tv.be_pred;
+                }
+            }
+        }
         double part[kNPart] = {};
 #pragma unroll 1
         for (int piece = 0; piece < (BATCH ? 2 : 1); ++piece) {
@@ -789,6 +906,8 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
             if (!ok) break;
             parity ^= 1;
             if (!(running > 0.0)) break;  // no CTA worked in this sweep: every image is done
+            if (prev_running >= 0.0 && running < prev_running) redeal = true;
+            prev_running = running;
             if (done) continue;
         } else {
             // four sums for CG, GD and Jacobi; PCG adds r.r
@@ -857,6 +976,17 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
             if (final_rep || (A.rtol > 0.0 && rel <= A.rtol) || it >= A.max_iters || !isfinite(rr_true)) {
                 if constexpr (BATCH) {
                     done = true;
+                    if ((int)blockIdx.x == lo && tid == 0) {  // the image's lead reports it now
+                        SolverOut* o = A.outs + img;
+                        o->status = (status == GM_OK && A.rtol > 0.0 && !(rel <= A.rtol)) ? GM_ERR_NOT_CONVERGED : status;
+                        o->iters = it;
+                        o->replacements = nrep;
+                        o->where = 0;
+                        o->rr_true = rr_true;
+                        o->bb = bb;
+                        o->rel = rel;
+                        A.img_done[img] = 1;
+                    }
                     continue;
                 } else {
                     break;
@@ -888,7 +1018,8 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
             }
         }
     }
-    const bool reporter = BATCH ? (img >= 0 && (int)blockIdx.x == lo) : blockIdx.x == 0;
+    // batched images report when they finish; here only those cut short
+    const bool reporter = BATCH ? (img >= 0 && !done && (int)blockIdx.x == lo) : blockIdx.x == 0;
     if (reporter && tid == 0) {
         SolverOut* o = BATCH ? A.outs + img : A.out;
         const int ab = ld_volatile_int(&A.gb->abort);

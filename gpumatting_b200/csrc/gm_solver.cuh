@@ -203,6 +203,8 @@ struct SolverArgs {
     // batched solves (BATCH kernels only)
     const BatchImage* imgs;
     const BatchUnit* units;  // [grid]
+    void* states;            // [nimg] solver state of each image, for re-deals
+    int* img_done;           // [nimg] set when an image has finished (zeroed before launch)
     int nimg;
     SolverOut* outs;         // [nimg]
 };

@@ -377,6 +377,14 @@ class LevinBatch:
         self._inputs[k] = (image, scribbles, gamma_map, s_map)
         return self
 
+    def restrict(self, k: int, scribbles=None, gamma_map=None, s_map=None, stream=None):
+        """gm_levin_restrict on image k's store view: its known pixels are
+        fixed and eliminated (hard constraints)."""
+        v = self.store_view(k)
+        sc = _scrib_desc(scribbles, 1.0, gamma_map, s_map)
+        L.check(L.load().gm_levin_restrict(C.byref(v), C.byref(sc), _stream(stream)))
+        return self
+
     def store_view(self, k: int) -> L.GmLevinStore:
         v = L.GmLevinStore()
         L.check(L.load().gm_batch_store(self.h, k, C.byref(v)))

@@ -138,13 +138,12 @@ struct SolverOut {
 
 // One image of a batched solve.  Images are stacked in one canvas, image k
 // occupying canvas rows y0 .. y0+H-1 (columns 0 .. W-1) with two zero rows
-// between neighbours; its units are CTAs c0 .. c0+units-1 (nstrips strips x
-// nseg row segments).
+// between neighbours; its CTAs are c0 .. c0+units-1 (their rows are in the
+// BatchUnit table).
 struct BatchImage {
     int y0, W, H;
-    int nstrips, nseg;
     int c0, units;
-    int pad_;
+    int pad_[3];
     float* alpha;             // [H][W] device: initial guess in, solution out
 };
 

@@ -80,16 +80,11 @@ def test_restricted_pcg_and_batch_view(orc):
     r = st.solve(alpha, "pcg", rtol=1e-10, max_iters=20000)
     assert r.status == 0, r
     assert np.abs(alpha.double().cpu().numpy().ravel() - x).max() <= 1e-4
-    from gpumatting_b200 import _lib as L
-    import ctypes as C
-
     b = api.LevinBatch([(W, H), (50, 40)], "fp16")
     b.assemble(0, img, scr, eps=p.eps)
     q = make_problem(50, 40, 9)
     b.assemble(1, torch.from_numpy(q.image).cuda(), torch.from_numpy(q.scribbles).cuda(), eps=q.eps)
-    view = b.store_view(0)
-    sc = api._scrib_desc(scr, 1.0, None, None)
-    L.check(L.load().gm_levin_restrict(C.byref(view), C.byref(sc), torch.cuda.current_stream().cuda_stream))
+    b.restrict(0, scribbles=scr)
     outs = [torch.full((H, W), 0.5, device="cuda"), torch.full((40, 50), 0.5, device="cuda")]
     res = b.solve(outs, "cg", rtol=1e-10, max_iters=20000, ctas_per_sm=3)
     assert all(r.status == 0 for r in res), res

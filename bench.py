@@ -15,6 +15,8 @@ relative residual 1e-6.
           RGB8 image, scribbles and initial alpha, assembly, solve, D2H alpha.
   plain   (N=1, rank 0) the plain FP32 method on the same image: 25-band FP32
           reference-layout store, fused CG, same stopping rule.
+  solvers (N=1, rank 0) CG, steepest descent and Jacobi to 1e-6, mixed and
+          plain, and CG / Jacobi PCG to 1e-10 (alpha within 1e-4 of FP64).
 
 Multi-GPU: one process per GPU (torchrun); every rank solves its own image
 (seed = rank), no data-path collective; time is the max over ranks.
@@ -41,7 +43,7 @@ METRIC = "Mpix·CG-iter/s and time to rel-residual 1e-6 at 1080p, mixed vs FP32,
 UNIT = "Mpix·CG-iter/s"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "source": "fallback"}
 
-# Algorithmic bytes per pixel (see DESIGN.md): Krylov sweep of the FP16
+# Algorithmic bytes per pixel: Krylov sweep of the FP16
 # symmetric store = 12 planes x 2 B + gamma 4 B + read r,q,p 12 B + write
 # r,p,q 12 B + solution increment read/write 8 B.
 KRYLOV_BYTES = {"fp16": 60, "bf16": 60, "fp32": 84, "ref25": 132}
@@ -391,6 +393,8 @@ def run_ours(args):
         if "pcg" in line:
             line["plain_fp32"]["speedup_mixed_pcg_vs_plain"] = (line["plain_fp32"]["ms_per_solve"]
                                                                 / line["pcg"]["ms_per_step"])
+    if rank == 0 and world == 1 and not args.no_solvers:
+        line["solvers"] = run_solvers(args, prob, img_d, scr_d, store, flush, stream)
     if args.batch_count > 0:
         line["batch"] = run_batch(args, stream, world, rank)
     if rank == 0 and world == 1 and args.large_size > 0:
@@ -631,6 +635,58 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
     return out
 
 
+def run_solvers(args, prob, img_d, scr_d, store, flush, stream) -> dict:
+    """The 1080p workload with every solver, mixed FP16 store against the plain
+    FP32 25-band store: CG, steepest descent and damped Jacobi (omega 2/3) to
+    true rel-res 1e-6, then CG and Jacobi PCG to 1e-10, the tolerance at which
+    alpha comes within 1e-4 of the FP64 solution (rel-res 1e-6 leaves every
+    solver, FP64 CG included, about 0.3 from it).  One solve per entry after
+    the headline's warm-up; L2 flushed before each."""
+    import torch
+
+    from gpumatting_b200 import api
+
+    W, H = prob.W, prob.H
+    N = W * H
+    alpha = torch.empty((H, W), dtype=torch.float32, device=img_d.device)
+    a, b = api.levin_bands25(img_d, scr_d, eps=prob.eps, gamma_value=100.0, arithmetic="fp64")
+    Lm = api.DeviceBandedMatrix(a, torch.tensor(api.levin_band_offsets(W), device=a.device), N)
+    x = api.PaddedVector(N, api.levin_pad(W))
+
+    def one(run, i):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return {"ms": e0.elapsed_time(e1), "iters": r.iters, "replacements": r.replacements,
+                "rel_residual": r.rel_residual, "status": r.status}
+
+    def mixed(solver, rtol, max_iters):
+        def run():
+            alpha.fill_(0.5)
+            return store.solve(alpha, solver, rtol=rtol, max_iters=max_iters, stream=stream)
+        return run
+
+    def plain(solver, rtol, max_iters):
+        def run():
+            x.data.fill_(0.5)
+            return api.banded_solve(Lm, x, b, W=W, solver=solver, rtol=rtol, max_iters=max_iters, replace_every=50)
+        return run
+
+    out = {"workload": f"{W}x{H} headline problem, alpha0 = 0.5, max 400000 iterations (GD, Jacobi) / 50000 (CG)"}
+    i = 0
+    for solver in ("cg", "gd", "jacobi"):
+        mi = 50000 if solver == "cg" else 400000
+        out[f"{solver}_1e-6"] = {"mixed_fp16": one(mixed(solver, 1e-6, mi), i), "plain_fp32": one(plain(solver, 1e-6, mi), i + 1)}
+        i += 2
+    # plain FP32 CG stalls near rel-res 1e-5 below 1e-6 (FP32 iterate); 10000 iterations show it
+    out["cg_1e-10"] = {"mixed_fp16": one(mixed("cg", 1e-10, 50000), i), "mixed_fp16_pcg": one(mixed("pcg", 1e-10, 50000), i + 1),
+                       "plain_fp32": one(plain("cg", 1e-10, 10000), i + 2)}
+    return out
+
+
 def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
     """Plain FP32 method: 25-band FP32 store + fused CG to 1e-6."""
     import numpy as np
@@ -678,6 +734,7 @@ def main():
     ap.add_argument("--solver", choices=["cg", "pcg"], default="cg",
                     help="solver of the headline step (profiling; the reported metric uses cg)")
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--no-solvers", action="store_true", help="skip the GD / Jacobi / tight-tolerance section")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)

@@ -214,7 +214,7 @@ struct KState {
 struct ImgState {
     KState s;
     int status, it, nrep, kind, final_rep, restart_due;
-    double rr_prev, bb, rr_true, rel, be_pred;
+    double rr_prev, bb, rr_true, rel, be_pred, jtol;
 };
 
 // Per-thread pipeline state that lives across sweeps: one bit per ring slot.
@@ -428,6 +428,9 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                 }
             }
         } else if (KIND == KIND_REPLACE) {
+            // Jacobi keeps its iterate in the FP32 vector (its sweeps read no
+            // FP64 base), so its fold goes back there with a zero base.
+            const bool jfold = MIXED && A.solver == GM_SOLVER_JACOBI;
             const float* vx = reinterpret_cast<const float*>(vsp + K.voff[1]);
             const float* vp = reinterpret_cast<const float*>(vsp + K.voff[2]);
             const float* vb = reinterpret_cast<const float*>(vsp + K.voff[3]);
@@ -459,16 +462,22 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             if (own_row) {
                 *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = ld2(vb, c);
                 if (in1) {
-                    if (MIXED) {
+                    if (MIXED && !jfold) {
                         *reinterpret_cast<double2*>(A.base[s.xsel ^ 1] + gi) = xf;
                         *reinterpret_cast<float2*>(A.xacc[s.xsel ^ 1] + gi) = make_float2(0.f, 0.f);
+                    } else if (MIXED) {
+                        *reinterpret_cast<double2*>(A.base[s.xsel ^ 1] + gi) = make_double2(0.0, 0.0);
+                        *reinterpret_cast<float2*>(A.xacc[s.xsel ^ 1] + gi) = make_float2((float)xf.x, (float)xf.y);
                     } else {
                         *reinterpret_cast<float2*>(A.xacc[s.xsel ^ 1] + gi) = make_float2((float)xf.x, (float)xf.y);
                     }
                 } else if (in0) {
-                    if (MIXED) {
+                    if (MIXED && !jfold) {
                         A.base[s.xsel ^ 1][gi] = xf.x;
                         A.xacc[s.xsel ^ 1][gi] = 0.f;
+                    } else if (MIXED) {
+                        A.base[s.xsel ^ 1][gi] = 0.0;
+                        A.xacc[s.xsel ^ 1][gi] = (float)xf.x;
                     } else {
                         A.xacc[s.xsel ^ 1][gi] = (float)xf.x;
                     }
@@ -816,6 +825,9 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
     KState s;
     s.af = 0.f; s.bf = 0.f; s.ad = 0.0; s.skipR = true; s.beta_zero = true; s.c = 0; s.xsel = 0;
     double rr_prev = 0.0, bb = -1.0, rr_true = 0.0, rel = 0.0, be_pred = 0.0;
+    // Jacobi: target of the in-sweep (FP32) residual; lowered when the FP64
+    // replacement finds the true residual still above rtol
+    double jtol = A.rtol;
     bool final_rep = false, restart_due = false;
     const bool gd = A.solver == GM_SOLVER_GD;
     const bool pcg_mode = A.solver == GM_SOLVER_PCG;
@@ -843,6 +855,7 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
                     t.s = s; t.status = status; t.it = it; t.nrep = nrep; t.kind = kind;
                     t.final_rep = final_rep; t.restart_due = restart_due;
                     t.rr_prev = rr_prev; t.bb = bb; t.rr_true = rr_true; t.rel = rel; t.be_pred = be_pred;
+                    t.jtol = jtol;
                     tab[img] = t;
                 }
                 ok = grid_sync(A.gb, G, A.limit_ns);
@@ -868,6 +881,7 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
                     s = tv.s; status = tv.status; it = tv.it; nrep = tv.nrep; kind = tv.kind;
                     final_rep = tv.final_rep != 0; restart_due = tv.restart_due != 0;
                     rr_prev = tv.rr_prev; bb = tv.bb; rr_true = tv.rr_true; rel = tv.rel; be_pred = tv.be_pred;
+                    jtol = tv.jtol;
                 }
             }
         }
@@ -992,6 +1006,13 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
                     break;
                 }
             }
+            if (jac) {
+                // the in-sweep residual met its target but the true one did
+                // not: go on iterating, aiming lower by the observed ratio
+                jtol *= 0.98 * A.rtol / rel;
+                kind = KIND_JACOBI;
+                continue;
+            }
             const bool bz = restart_due || gd || !(rr_prev > 0.0);
             // after a replacement CG rescales with the true residual; PCG keeps
             // the predicted r.z ratio (the replacement sweep has no diagonal)
@@ -1011,9 +1032,10 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
                 if (!(bb > 0.0)) bb = tot[0] > 0.0 ? tot[0] : 1.0;
             }
             const double rl = sqrt(tot[0] / bb);
-            if ((A.rtol > 0.0 && rl <= A.rtol) || it >= A.max_iters || !isfinite(tot[0])) {
+            if ((A.rtol > 0.0 && rl <= jtol) || it >= A.max_iters || !isfinite(tot[0])) {
+                // the replacement sweep checks the true residual in FP64
                 kind = KIND_REPLACE;
-                final_rep = true;
+                final_rep = it >= A.max_iters || !isfinite(tot[0]);
                 s.ad = 0.0; s.af = 0.f;
             }
         }

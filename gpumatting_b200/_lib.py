@@ -24,7 +24,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "UNSUPPORTED", 4: "TIMEOUT"
                 6: "NOT_CONVERGED", 7: "NOMEM"}
 
 GM_PREC_FP32, GM_PREC_FP16, GM_PREC_BF16 = 0, 1, 2
-GM_SOLVER_CG, GM_SOLVER_GD, GM_SOLVER_JACOBI, GM_SOLVER_PCG = 0, 1, 2, 3
+GM_SOLVER_CG, GM_SOLVER_GD, GM_SOLVER_JACOBI, GM_SOLVER_PCG, GM_SOLVER_MG = 0, 1, 2, 3, 4
 GM_IMAGE_RGB8, GM_IMAGE_RGBA32F = 0, 1
 GM_ASSEMBLY_FP64, GM_ASSEMBLY_REFERENCE = 0, 1
 
@@ -58,7 +58,8 @@ class GmLevinStore(C.Structure):
 class GmSolveParams(C.Structure):
     _fields_ = [("solver", C.c_int), ("rtol", C.c_double), ("max_iters", C.c_int), ("restart", C.c_int),
                 ("replace_every", C.c_int), ("omega", C.c_float), ("use_low", C.c_int), ("timeout_s", C.c_double),
-                ("ctas_per_sm", C.c_int), ("strip_width", C.c_int), ("inject", C.c_int)]
+                ("ctas_per_sm", C.c_int), ("strip_width", C.c_int), ("inject", C.c_int), ("mg_omega", C.c_float),
+                ("mg_scale", C.c_float)]
 
 
 class GmSolveInfo(C.Structure):
@@ -131,6 +132,8 @@ SIGNATURES = {
                               C.POINTER(GmSolveInfo), _vp]),
     "gm_banded_solve": (_i, [BandedMatrix, _i, _vp, _i, _vp, C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo),
                              _vp]),
+    "gm_levin_mg_levels": (_i, [_i, _i, C.POINTER(C.c_int), C.POINTER(C.c_int), _i]),
+    "gm_levin_mg_inspect": (_i, [C.POINTER(GmLevinStore), _i, _vp, _vp, _i, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -196,7 +196,8 @@ def compute_error(alpha, gt, W: int, H: int, stream=None) -> float:
 # Native: symmetric Levin store
 # ---------------------------------------------------------------------------
 PRECISIONS = {"fp32": L.GM_PREC_FP32, "fp16": L.GM_PREC_FP16, "bf16": L.GM_PREC_BF16}
-SOLVERS = {"cg": L.GM_SOLVER_CG, "gd": L.GM_SOLVER_GD, "jacobi": L.GM_SOLVER_JACOBI, "pcg": L.GM_SOLVER_PCG}
+SOLVERS = {"cg": L.GM_SOLVER_CG, "gd": L.GM_SOLVER_GD, "jacobi": L.GM_SOLVER_JACOBI, "pcg": L.GM_SOLVER_PCG,
+           "mg": L.GM_SOLVER_MG}
 
 
 def _image_desc(image) -> L.GmImage:
@@ -296,6 +297,31 @@ class LevinStore:
             L.check(rc)
         return SolveResult.from_info(info)
 
+    def mg_levels(self) -> list:
+        """(width, height) of each level of the GM_SOLVER_MG hierarchy."""
+        n = C.c_int(0)
+        dims = (C.c_int * 64)()
+        L.check(L.load().gm_levin_mg_levels(self.W, self.H, C.byref(n), dims, 32))
+        return [(dims[2 * i], dims[2 * i + 1]) for i in range(n.value)]
+
+    def mg_inspect(self, r=None, level: int = 0, use_low: bool = True, stream=None):
+        """Builds the multigrid hierarchy; returns (z, c, D): z = one V-cycle
+        applied to r ([H, W] device floats, or None), and for level >= 1 that
+        level's coupling planes (4, H_l, W_l) and diagonal (H_l, W_l) as numpy
+        arrays (None for level 0)."""
+        import numpy as np
+
+        torch = _torch()
+        z = None if r is None else torch.empty_like(r)
+        c = d = None
+        if level >= 1:
+            Wl, Hl = self.mg_levels()[level]
+            c = np.zeros((4, Hl, Wl), np.float32)
+            d = np.zeros((Hl, Wl), np.float32)
+        L.check(L.load().gm_levin_mg_inspect(C.byref(self.s), 1 if use_low else 0, _ptr(r), _ptr(z), level,
+                                             None if c is None else c.ctypes.data,
+                                             None if d is None else d.ctypes.data, _stream(stream)))
+        return z, c, d
 
     def apply(self, x, y=None, true_op: bool = False, stream=None):
         """y = A x ([H, W'] device floats, W' >= W a multiple of 4) with the

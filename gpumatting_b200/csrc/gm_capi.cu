@@ -71,8 +71,8 @@ extern "C" int gm_banded_solve(BandedMatrix L, int W, float* alpha, int pad, con
     if (prm) p = *prm; else gm_default_params(&p);
     cudaStream_t st = (cudaStream_t)stream;
     if (!alpha || !b || !L.a || L.rows <= 0) { gm_set_error_msg("gm_banded_solve: bad arguments"); return GM_ERR_INVALID; }
-    if (p.solver == GM_SOLVER_PCG) {
-        gm_set_error_msg("GM_SOLVER_PCG runs on the symmetric Levin store (gm_levin_solve), not on 25 bands");
+    if (p.solver == GM_SOLVER_PCG || p.solver == GM_SOLVER_MG) {
+        gm_set_error_msg("GM_SOLVER_PCG / GM_SOLVER_MG run on the symmetric Levin store (gm_levin_solve), not on 25 bands");
         return GM_ERR_UNSUPPORTED;
     }
     std::vector<int> offs;
@@ -131,6 +131,7 @@ static int levin_solve_impl(const gm_levin_store* store, const float* b, int bpi
     gm_solve_params p;
     if (prm) p = *prm; else gm_default_params(&p);
     if (!store || !store->w32 || !alpha || !b) { gm_set_error_msg("gm_levin_solve: bad arguments"); return GM_ERR_INVALID; }
+    if (p.solver == GM_SOLVER_MG) return run_mg_solver(store, b, bpitch, alpha, alpha, &p, info, (cudaStream_t)stream);
     const int W = store->W, H = store->H, P = store->pitch;
     SolverSetup S;
     memset(&S, 0, sizeof(S));

@@ -39,4 +39,9 @@ struct SolverSetup {
 
 int run_solver(const SolverSetup& S, const gm_solve_params* p, gm_solve_info* info, cudaStream_t st);
 
+// Multigrid-preconditioned CG on the symmetric store (gm_mg.cu): b is
+// [H][bpitch], alpha_in / alpha_out [H][W] (may alias).
+int run_mg_solver(const gm_levin_store* store, const float* b, int bpitch, const float* alpha_in, float* alpha_out,
+                  const gm_solve_params* p, gm_solve_info* info, cudaStream_t st);
+
 }  // namespace gm

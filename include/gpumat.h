@@ -162,8 +162,16 @@ int gm_compute_error(double* mse_host, const float* alpha, const float* gt, int 
 enum { GM_PREC_FP32 = 0, GM_PREC_FP16 = 1, GM_PREC_BF16 = 2 };
 /* GM_SOLVER_PCG: CG preconditioned with the operator's diagonal (Jacobi);
  * symmetric store only (gm_levin_solve*, batches).  No counterpart in the
- * reference, whose cgSolve is unpreconditioned. */
-enum { GM_SOLVER_CG = 0, GM_SOLVER_GD = 1, GM_SOLVER_JACOBI = 2, GM_SOLVER_PCG = 3 };
+ * reference, whose cgSolve is unpreconditioned.
+ * GM_SOLVER_MG: CG preconditioned with an aggregation multigrid V-cycle
+ * (2x2 piecewise-constant aggregates, Galerkin coarse operators, one damped
+ * Jacobi step before and after each coarse correction, exact solve of the
+ * coarsest level of <= 128 cells); single symmetric-store solves only
+ * (gm_levin_solve, gm_levin_solve_rhs, gm_levin_adjoint).  The reference
+ * sketches aggregation operators over superpixels for this purpose
+ * (gridoperators.h:18-138, SLIC.cpp:32, commented out at main.cu:201-218)
+ * without finishing them. */
+enum { GM_SOLVER_CG = 0, GM_SOLVER_GD = 1, GM_SOLVER_JACOBI = 2, GM_SOLVER_PCG = 3, GM_SOLVER_MG = 4 };
 enum { GM_IMAGE_RGB8 = 0, GM_IMAGE_RGBA32F = 1 };
 /* Assembly arithmetic: FP64 throughout (rounded once), or the reference's
  * float/double mix (bit-identical to hostLevinLaplacian). */
@@ -250,6 +258,8 @@ typedef struct gm_solve_params_s {
     int inject;           /* test hook, 0 in normal use: 1 = the first grid barrier
                              waits for one arrival that never comes, so the call
                              must end with GM_ERR_TIMEOUT after timeout_s */
+    float mg_omega;       /* GM_SOLVER_MG: smoother damping (0 = 0.8)      */
+    float mg_scale;       /* GM_SOLVER_MG: coarse-correction scale (0 = 1.8) */
 } gm_solve_params;
 
 typedef struct gm_solve_info_s {
@@ -301,6 +311,20 @@ int gm_levin_adjoint(const gm_levin_store* st, const gm_image* im, const gm_scri
                      const float* alpha, const float* dalpha, float* lambda, float* dimage,
                      size_t dimage_pitch, int dimage_channels, float* dgamma, const gm_solve_params* p,
                      gm_solve_info* info, void* stream);
+
+/* Level shapes of the GM_SOLVER_MG hierarchy for a W x H image: *nlevels
+ * levels, dims[2l], dims[2l+1] = width, height of level l (up to cap). */
+int gm_levin_mg_levels(int W, int H, int* nlevels, int* dims, int cap);
+
+/* Builds the GM_SOLVER_MG hierarchy of an assembled store (use_low: on the
+ * low-precision planes, as the solver does) and, when r and z are given,
+ * applies ONE V-cycle z = M^-1 r (device [H][W] floats).  When level >= 1 and
+ * c_host / d_host are given, copies that level's 4 coupling planes (E, SW, S,
+ * SE; [4][H_l][W_l]) and diagonal ([H_l][W_l]) to host memory.  For tests and
+ * diagnostics of the preconditioner (the aggregation operators of
+ * gridoperators.h:18-138, here on 2x2 blocks). */
+int gm_levin_mg_inspect(const gm_levin_store* st, int use_low, const float* r, float* z, int level,
+                        float* c_host, float* d_host, void* stream);
 
 /* ------------------------------------------------------------------ */
 /* Data formats either side of the solve                               */

@@ -1,0 +1,173 @@
+"""Multigrid-preconditioned CG (GM_SOLVER_MG) on the GPU against the FP64
+oracle of oracle/mg.py: the Galerkin hierarchy level by level, one V-cycle,
+solves to rel-res 1e-6 (FP16, BF16, FP32 stores) and 1e-10 (alpha within
+1e-4 of the direct FP64 solve), determinism, odd shapes, and the status
+paths.  The hierarchy is the 2x2-aggregate form of the reference's
+unfinished aggregation operators (gridoperators.h:18-138)."""
+import numpy as np
+import pytest
+
+from gpu_util import oracle_problem, torch_cuda
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def _store(orc, W, H, prec, seed=2):
+    torch = torch_cuda()
+    from gpumatting_b200 import api
+
+    p, w, g, b = oracle_problem(orc, W, H, seed)
+    st = api.LevinStore(W, H, prec).assemble(torch.from_numpy(p.image).cuda(), torch.from_numpy(p.scribbles).cuda(),
+                                             eps=p.eps, gamma_value=100.0)
+    return st, p, w, g, b
+
+
+def _oracle_levels(st, g, prec, use_low=True):
+    from oracle import mg as M
+
+    W, H = st.W, st.H
+    low = use_low and prec != "fp32"
+    wp = st.planes("w" if low else "w32")[:, :, :W].reshape(12, -1).double().cpu().numpy()
+    dp = st.planes("d" if low else "d32")[:, :W].reshape(-1).double().cpu().numpy()
+    return M, M.hierarchy(wp, dp, g, W, H)
+
+
+def _true_relres(orc, st, g, b, x):
+    W, H = st.W, st.H
+    w32 = st.planes("w32")[:, :, :W].reshape(12, -1).double().cpu().numpy()
+    op = orc.Operator(W=W, H=H, w=w32, gamma=g)
+    return np.linalg.norm(b - op.apply(x)) / np.linalg.norm(b), op
+
+
+@pytest.mark.parametrize("W,H,prec", [(160, 120, "fp16"), (37, 29, "fp32"), (300, 17, "bf16")])
+def test_hierarchy_matches_oracle(orc, W, H, prec):
+    st, p, w, g, b = _store(orc, W, H, prec)
+    M, lv = _oracle_levels(st, g, prec)
+    assert st.mg_levels() == [(l.W, l.H) for l in lv]
+    for level in sorted({1, len(lv) - 1}):
+        _, c, D = st.mg_inspect(None, level)
+        ref = lv[level]
+        scale = np.abs(ref.c).max()
+        assert np.allclose(c, ref.c, rtol=1e-5, atol=1e-6 * scale), level
+        assert np.allclose(D, ref.D, rtol=1e-5, atol=1e-6 * np.abs(ref.D).max()), level
+
+
+@pytest.mark.parametrize("prec", ["fp16", "fp32"])
+def test_vcycle_matches_oracle(orc, prec):
+    torch = torch_cuda()
+    W, H = 200, 150
+    st, p, w, g, b = _store(orc, W, H, prec)
+    M, lv = _oracle_levels(st, g, prec)
+    r = np.random.default_rng(7).standard_normal((H, W)).astype(np.float32)
+    z, _, _ = st.mg_inspect(torch.from_numpy(r).cuda(), 0)
+    ref = M.vcycle(lv, r.astype(np.float64))
+    err = np.linalg.norm(z.double().cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err <= 1e-4, err
+
+
+@pytest.mark.parametrize("prec", ["fp16", "bf16", "fp32"])
+def test_mg_solve_to_rtol(orc, prec):
+    torch = torch_cuda()
+    W, H = 160, 120
+    st, p, w, g, b = _store(orc, W, H, prec)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    res = st.solve(alpha, "mg", rtol=1e-6, max_iters=2000)
+    assert res.status == 0 and res.rel_residual <= 1e-6, res
+    rel, op = _true_relres(orc, st, g, b, alpha.double().cpu().numpy().ravel())
+    assert rel <= 1.05e-6
+    M, lv = _oracle_levels(st, g, prec)
+    _, it64, _ = M.mgpcg(lv, op.apply, b, np.full(W * H, 0.5), 1e-6, 2000)
+    assert res.iters <= 1.3 * it64 + 10, (res.iters, it64)
+    _, it_cg, _ = op.cg(b, np.full(W * H, 0.5), rtol=1e-6, maxit=20000)
+    assert 4 * res.iters < it_cg, (res.iters, it_cg)
+
+
+def test_mg_accurate_vs_direct(orc):
+    """rtol 1e-10: alpha within 1e-4 max-abs of the FP64 direct solve."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    torch = torch_cuda()
+    W, H = 64, 48
+    st, p, w, g, b = _store(orc, W, H, "fp16", seed=5)
+    a = orc.sym_to_bands64(w, g, W, H)
+    offs = orc.levin_offsets(W)
+    N = W * H
+    rows, cols, vals = [], [], []
+    for k in range(25):
+        i = np.arange(N)
+        j = i + offs[k]
+        m = (j >= 0) & (j < N) & (a[k] != 0)
+        rows.append(i[m]); cols.append(j[m]); vals.append(a[k][m])
+    Mx = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+    xs = spla.spsolve(Mx.tocsc(), b)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    res = st.solve(alpha, "mg", rtol=1e-10, max_iters=5000)
+    assert res.status == 0 and res.rel_residual <= 1e-10, res
+    assert np.abs(alpha.double().cpu().numpy().ravel() - xs).max() <= TOL
+
+
+def test_mg_is_deterministic(orc):
+    torch = torch_cuda()
+    W, H = 300, 200
+    st, p, w, g, b = _store(orc, W, H, "fp16")
+    outs = []
+    for _ in range(2):
+        alpha = torch.full((H, W), 0.5, device="cuda")
+        res = st.solve(alpha, "mg", rtol=0.0, max_iters=25)
+        assert res.iters == 25 and res.status == 0
+        outs.append(alpha.cpu().numpy())
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("W,H", [(8, 2), (5, 7), (97, 61), (130, 3)])
+def test_mg_odd_shapes(orc, W, H):
+    torch = torch_cuda()
+    st, p, w, g, b = _store(orc, W, H, "fp16", seed=1)
+    if not np.any(b):
+        pytest.skip("no foreground scribble at this size")
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    res = st.solve(alpha, "mg", rtol=1e-6, max_iters=2000)
+    assert res.status == 0, res
+    rel, _ = _true_relres(orc, st, g, b, alpha.double().cpu().numpy().ravel())
+    assert rel <= 1.05e-6
+
+
+def test_mg_zero_rhs_and_max_iters(orc):
+    torch = torch_cuda()
+    W, H = 96, 64
+    st, p, w, g, b = _store(orc, W, H, "fp16")
+    x = torch.full((H, W), 0.25, device="cuda")
+    res = st.solve_rhs(torch.zeros((H, W), device="cuda"), x, "mg", rtol=1e-6)
+    assert res.status == 0 and not x.any()
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    res = st.solve(alpha, "mg", rtol=1e-30, max_iters=3)
+    assert res.status == 6 and res.iters == 3  # NOT_CONVERGED, and the iterate is still written
+    assert np.isfinite(alpha.cpu().numpy()).all()
+
+
+def test_mg_adjoint_matches_cg_adjoint(orc):
+    torch = torch_cuda()
+    W, H = 96, 64
+    st, p, w, g, b = _store(orc, W, H, "fp16")
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    st.solve(alpha, "cg", rtol=1e-9, max_iters=20000)
+    gt = torch.from_numpy(p.alpha_gt.astype(np.float32)).cuda()
+    dalpha = 2.0 * (alpha - gt) / (W * H)
+    d_cg, dg_cg, lam_cg, r_cg = st.adjoint(alpha, dalpha, "cg", rtol=1e-9, max_iters=20000)
+    d_mg, dg_mg, lam_mg, r_mg = st.adjoint(alpha, dalpha, "mg", rtol=1e-9, max_iters=2000)
+    assert r_mg.status == 0 and r_mg.iters * 4 < r_cg.iters, (r_mg, r_cg)
+    for a_, b_ in ((lam_mg, lam_cg), (d_mg, d_cg), (dg_mg, dg_cg)):
+        a_, b_ = a_.double().cpu().numpy(), b_.double().cpu().numpy()
+        assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_)
+
+
+def test_mg_rejected_where_unsupported(orc):
+    torch = torch_cuda()
+    from gpumatting_b200 import _lib as L
+    from gpumatting_b200 import api
+
+    batch = api.LevinBatch([(64, 48)], "fp16")
+    with pytest.raises(L.GmError):
+        batch.solve([torch.full((48, 64), 0.5, device="cuda")], "mg")

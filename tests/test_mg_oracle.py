@@ -1,0 +1,63 @@
+"""CPU checks of the multigrid oracle (oracle/mg.py) that the GPU hierarchy,
+V-cycle and solve are compared with.  The reference leaves its aggregation
+operators unfinished (gridoperators.h:18-138), so there is no reference
+output to pin against; the oracle is pinned by identities instead: each
+coarse operator equals P^T A P, the V-cycle is a symmetric positive-definite
+operator, and PCG with it converges on the synthetic problems."""
+import numpy as np
+import pytest
+
+from gpumatting_b200.synth import make_problem
+
+
+def _levels(orc, W, H, seed=0):
+    from oracle import mg as M
+
+    p = make_problem(W, H, seed)
+    w = orc.levin_sym64(p.image.astype(np.float64) / 255.0, p.eps)
+    g = p.gamma.ravel().astype(np.float64)
+    d = g.reshape(H, W).copy()
+    for k, (du, dv) in enumerate(M.fine_offsets()):
+        wk = w[k].reshape(H, W)
+        d += wk + M._shift(wk, -du, -dv)
+    return M, p, w, g, d.ravel(), M.hierarchy(w, d.ravel(), g, W, H)
+
+
+@pytest.mark.parametrize("W,H", [(40, 30), (37, 29), (9, 14)])
+def test_level_zero_is_the_operator_and_coarse_levels_are_galerkin(orc, W, H):
+    M, p, w, g, d, lv = _levels(orc, W, H)
+    op = orc.Operator(W=W, H=H, w=w, gamma=g)
+    x = np.random.default_rng(0).standard_normal(W * H)
+    assert np.allclose(lv[0].apply(x.reshape(H, W)).ravel(), op.apply(x), rtol=1e-12, atol=1e-9)
+    for l in range(len(lv) - 1):
+        f, c = lv[l], lv[l + 1]
+        assert (c.W, c.H) == ((f.W + 1) // 2, (f.H + 1) // 2)
+        xc = np.random.default_rng(l).standard_normal((c.H, c.W))
+        lhs = c.apply(xc)
+        rhs = M.restrict(f.apply(M.prolong(xc, f.H, f.W)), c.H, c.W)
+        assert np.allclose(lhs, rhs, rtol=1e-10, atol=1e-9 * np.abs(lhs).max())
+    assert lv[-1].W * lv[-1].H <= M.COARSE_MAX < lv[-2].W * lv[-2].H or len(lv) == 2
+    n = lv[-1].W * lv[-1].H
+    assert np.allclose(lv[-1].inv @ lv[-1].A, np.eye(n), atol=1e-8)
+
+
+def test_vcycle_is_symmetric_positive_definite(orc):
+    M, p, w, g, d, lv = _levels(orc, 48, 36)
+    rng = np.random.default_rng(3)
+    u, v = rng.standard_normal((2, 36, 48))
+    Mu, Mv = M.vcycle(lv, u), M.vcycle(lv, v)
+    assert abs(np.sum(u * Mv) - np.sum(Mu * v)) <= 1e-10 * np.sqrt(np.sum(u * u) * np.sum(Mv * Mv))
+    for t in (u, v):
+        assert np.sum(t * M.vcycle(lv, t)) > 0.0
+
+
+def test_mgpcg_converges_and_beats_cg(orc):
+    W, H = 160, 120
+    M, p, w, g, d, lv = _levels(orc, W, H)
+    op = orc.Operator(W=W, H=H, w=w, gamma=g)
+    b = (p.gamma * p.s).ravel().astype(np.float64)
+    x, it, rel = M.mgpcg(lv, op.apply, b, np.full(W * H, 0.5), 1e-6, 400)
+    assert rel <= 1e-6
+    assert np.linalg.norm(b - op.apply(x.ravel())) / np.linalg.norm(b) <= 1.001e-6
+    _, it_cg, _ = op.cg(b, np.full(W * H, 0.5), rtol=1e-6, maxit=20000)
+    assert it * 4 < it_cg, (it, it_cg)

@@ -15,8 +15,11 @@ relative residual 1e-6.
           RGB8 image, scribbles and initial alpha, assembly, solve, D2H alpha.
   plain   (N=1, rank 0) the plain FP32 method on the same image: 25-band FP32
           reference-layout store, fused CG, same stopping rule.
+  pcg, mg (N=1, rank 0) the same step with Jacobi-preconditioned CG and with
+          the multigrid-preconditioned CG.
   solvers (N=1, rank 0) CG, steepest descent and Jacobi to 1e-6, mixed and
-          plain, and CG / Jacobi PCG to 1e-10 (alpha within 1e-4 of FP64).
+          plain, and CG / Jacobi PCG / multigrid PCG to 1e-10 (alpha within
+          1e-4 of FP64).
 
 Multi-GPU: one process per GPU (torchrun); every rank solves its own image
 (seed = rank), no data-path collective; time is the max over ranks.
@@ -387,12 +390,35 @@ def run_ours(args):
                        "rel_residual_max": max(r.rel_residual for r in res_p),
                        "mpix_iter_s": N * it_p / 1e6 / (sum(ms_p) / 1000),
                        "solver_kernel_ms": sum(r.kernel_ms for r in res_p) / args.steps}
+    if rank == 0 and world == 1 and not args.no_mg:
+        # the same step with the multigrid-preconditioned CG, to the same true rel-res
+        def step_mg():
+            store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
+            alpha.copy_(a0_d, non_blocking=True)
+            return store.solve(alpha, "mg", **params)
+
+        for _ in range(2):
+            step_mg()
+        ms_m, res_m = timed(step_mg, args.steps)
+        assert all(r.status == 0 and (args.fixed_iters or r.rel_residual <= 1e-6) for r in res_m), res_m
+        it_m = sum(r.iters for r in res_m)
+        line["mg"] = {"solver": "multigrid-preconditioned CG (2x2 aggregation V-cycle on the FP16 planes, FP32 "
+                                "outer operator, FP64 solution and replacement every 50), one graph launch per solve",
+                      "ms_per_step": sum(ms_m) / args.steps, "iters_per_solve": it_m / args.steps,
+                      "levels": res_m[0].grid,
+                      "replacements_per_solve": sum(r.replacements for r in res_m) / args.steps,
+                      "rel_residual_max": max(r.rel_residual for r in res_m),
+                      "solve_ms": sum(r.kernel_ms for r in res_m) / args.steps,
+                      "speedup_vs_cg": (1000 * t_max / args.steps) / (sum(ms_m) / args.steps)}
     if rank == 0 and world == 1 and not args.no_plain:
         line["plain_fp32"] = run_plain(args, prob, img_d, scr_d, flush, stream)
         line["plain_fp32"]["speedup_mixed_vs_plain"] = line["plain_fp32"]["ms_per_solve"] / line["ms_per_step"]
         if "pcg" in line:
             line["plain_fp32"]["speedup_mixed_pcg_vs_plain"] = (line["plain_fp32"]["ms_per_solve"]
                                                                 / line["pcg"]["ms_per_step"])
+        if "mg" in line:
+            line["plain_fp32"]["speedup_mixed_mg_vs_plain"] = (line["plain_fp32"]["ms_per_solve"]
+                                                               / line["mg"]["ms_per_step"])
     if rank == 0 and world == 1 and not args.no_solvers:
         line["solvers"] = run_solvers(args, prob, img_d, scr_d, store, flush, stream)
     if args.batch_count > 0:
@@ -478,8 +504,14 @@ def run_large(args, stream, peaks) -> dict:
         torch.cuda.synchronize()
     out.update({"pcg_status": rp.status, "pcg_iters": rp.iters, "pcg_rel_residual": rp.rel_residual,
                 "pcg_solve_kernel_ms": rp.kernel_ms})
+    for rep in range(2):
+        alpha.fill_(0.5)
+        rm = st.solve(alpha, "mg", rtol=1e-6, max_iters=5000, stream=stream)
+        torch.cuda.synchronize()
+    out.update({"mg_status": rm.status, "mg_iters": rm.iters, "mg_rel_residual": rm.rel_residual,
+                "mg_solve_ms": rm.kernel_ms})
     dalpha = 2.0 * (alpha - gt) / N
-    for solver in ("cg", "pcg"):
+    for solver in ("cg", "pcg", "mg"):
         for rep in range(2):
             e0, e1 = ev()
             e0.record(stream)
@@ -487,7 +519,7 @@ def run_large(args, stream, peaks) -> dict:
                                                  stream=stream)
             e1.record(stream)
             torch.cuda.synchronize()
-        key = "adjoint" if solver == "cg" else "adjoint_pcg"
+        key = "adjoint" if solver == "cg" else "adjoint_" + solver
         out.update({f"{key}_ms": e0.elapsed_time(e1), f"{key}_status": ra.status, f"{key}_iters": ra.iters,
                     f"{key}_rel_residual": ra.rel_residual, f"{key}_solve_kernel_ms": ra.kernel_ms,
                     f"{key}_backprop_ms": e0.elapsed_time(e1) - ra.kernel_ms,
@@ -683,7 +715,8 @@ def run_solvers(args, prob, img_d, scr_d, store, flush, stream) -> dict:
         i += 2
     # plain FP32 CG stalls near rel-res 1e-5 below 1e-6 (FP32 iterate); 10000 iterations show it
     out["cg_1e-10"] = {"mixed_fp16": one(mixed("cg", 1e-10, 50000), i), "mixed_fp16_pcg": one(mixed("pcg", 1e-10, 50000), i + 1),
-                       "plain_fp32": one(plain("cg", 1e-10, 10000), i + 2)}
+                       "mixed_fp16_mg": one(mixed("mg", 1e-10, 5000), i + 2),
+                       "plain_fp32": one(plain("cg", 1e-10, 10000), i + 3)}
     return out
 
 
@@ -731,7 +764,8 @@ def main():
     ap.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-pcg", action="store_true", help="skip the Jacobi-preconditioned comparison")
-    ap.add_argument("--solver", choices=["cg", "pcg"], default="cg",
+    ap.add_argument("--no-mg", action="store_true", help="skip the multigrid-preconditioned comparison")
+    ap.add_argument("--solver", choices=["cg", "pcg", "mg"], default="cg",
                     help="solver of the headline step (profiling; the reported metric uses cg)")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-solvers", action="store_true", help="skip the GD / Jacobi / tight-tolerance section")

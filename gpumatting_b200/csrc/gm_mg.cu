@@ -86,6 +86,7 @@ struct Lev {
     void* c;              // planes [NP][H][P] (level 0: the store's w, type T)
     size_t ps;            // plane stride (elements)
     float* D;             // diagonal [H][P]
+    float* Di;            // 1 / D (0 where D = 0): the smoothers multiply
     float* gam;           // summed scribble weight (l >= 1)
     float* b;             // right-hand side of the V-cycle on this level
     float* x;             // V-cycle result on this level
@@ -94,6 +95,7 @@ struct Lev {
 struct Args {
     Lev lev[kMaxLevels];
     int L;                // index of the coarsest level
+    int lt;               // first level of the single-CTA tail (1 <= lt <= L)
     int W, H, P;          // fine grid (== lev[0])
     const float* w32;     // true operator: FP32 planes, gamma and d32 = gamma + row sum
     size_t ps32;
@@ -119,6 +121,19 @@ struct Args {
 // ---------------------------------------------------------------------------
 
 template <class T> __device__ __forceinline__ float tof(T v) { return Cvt<T>::to_f(v); }
+
+// Programmatic dependent launch: every kernel of the solve is launched with
+// programmatic stream serialisation, lets its successor start launching at
+// once, and waits for its predecessor's completion (and memory) before its
+// first access.  This hides the launch gap between the many short kernels of
+// a V-cycle.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter()
+{
+    pdl_wait();
+    pdl_trigger();
+}
 
 // Plane tile: NP planes x ROWS rows (y0 - 2 .. y0 + ROWS - 3) x kPW columns
 // starting at x0 - 8 (16-byte aligned: x0 is a multiple of 64 and P of 8).
@@ -190,7 +205,7 @@ __device__ __forceinline__ void fill_tile(float* vt, int P, int W, int H, int x0
 template <int NV>
 __device__ __forceinline__ bool last_cta_total(double (&v)[NV], double* parts, unsigned* ticket)
 {
-    __shared__ double red[(kThreads / 32) * NV + NV];
+    __shared__ double red[32 * NV + NV];
     __shared__ int s_last;
     block_sum<NV>(v, red);
     const unsigned G = gridDim.x;
@@ -207,11 +222,11 @@ __device__ __forceinline__ bool last_cta_total(double (&v)[NV], double* parts, u
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (wid < NV) {
         const double t = warp_sum_range(parts + (size_t)wid * kMaxParts, 0, (int)G);
-        if (lane == 0) red[(kThreads / 32) * NV + wid] = t;
+        if (lane == 0) red[32 * NV + wid] = t;
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = red[(kThreads / 32) * NV + k];
+    for (int k = 0; k < NV; ++k) v[k] = red[32 * NV + k];
     if (threadIdx.x == 0) *ticket = 0u;
     return true;
 }
@@ -222,16 +237,20 @@ __device__ __forceinline__ void set_cond(const Args& a, unsigned v)
 }
 
 // ---------------------------------------------------------------------------
-// Stencil application on shared-memory tiles.
+// Stencil sums on shared-memory tiles.
 // vt: vector tile with origin (x0 - 2, y0 - 2), width kVW; pt: plane tile
 // with origin (x0 - 8, y0 - 2), width kPW, `prow` rows per plane.
-// Returns d * v_i - sum_j w_ij v_j at tile-local output (lx, ly).
+// Returns S_i = sum_j w_ij v_j at tile-local output (lx, ly), so that
+// (A v)_i = D_i v_i - S_i.  With x1 = omega b / D the smoother steps become
+//   rho = b - A x1 = (1 - omega) b + S(x1)          (D > 0; rho = b + S if D = 0)
+//   x = y + omega (b - A y) / D = (1 - omega) y + omega (b + S(y)) / D
+// which need only 1 / D.
 // ---------------------------------------------------------------------------
 template <class S, class T>
-__device__ __forceinline__ float sten_apply(const T* pt, int prow, const float* vt, float dval, int lx, int ly)
+__device__ __forceinline__ float sten_sum(const T* pt, int prow, const float* vt, int lx, int ly)
 {
     const int vc = (ly + kHalo) * kVW + lx + kHalo;
-    float a0 = dval * vt[vc], a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
     for (int k = 0; k < S::NP; ++k) {
         const int du = S::du(k), dv = S::dv(k);
@@ -239,10 +258,19 @@ __device__ __forceinline__ float sten_apply(const T* pt, int prow, const float* 
         const float wl = tof(pt[((size_t)k * prow + ly + kHalo - dv) * kPW + lx + 8 - du]);
         const float xu = vt[vc + dv * kVW + du];
         const float xl = vt[vc - dv * kVW - du];
-        if (k & 1) { a1 = fmaf(-wu, xu, a1); a3 = fmaf(-wl, xl, a3); }
-        else { a2 = fmaf(-wu, xu, a2); a0 = fmaf(-wl, xl, a0); }
+        if (k & 1) { a1 = fmaf(wu, xu, a1); a3 = fmaf(wl, xl, a3); }
+        else { a2 = fmaf(wu, xu, a2); a0 = fmaf(wl, xl, a0); }
     }
     return (a0 + a2) + (a1 + a3);
+}
+
+__device__ __forceinline__ float rho_of(float b, float di, float om, float S)
+{
+    return (di > 0.f ? (1.f - om) * b : b) + S;
+}
+__device__ __forceinline__ float smooth_of(float y, float b, float di, float om, float S)
+{
+    return di > 0.f ? fmaf(om * di, b + S, (1.f - om) * y) : y;
 }
 
 // ---------------------------------------------------------------------------
@@ -255,6 +283,7 @@ __device__ __forceinline__ float sten_apply(const T* pt, int prow, const float* 
 // W are written as zero and left out of the sum.
 __global__ void __launch_bounds__(kThreads) mg_update_kernel(Args a)
 {
+    pdl_enter();
     State* st = a.st;
     if (st->done) return;
     const int W = a.W, H = a.H, P = a.P;
@@ -302,6 +331,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(Args a)
 // only when a replacement is due).  Also forms ||b||^2 on the first call.
 __global__ void __launch_bounds__(kThreads, 3) mg_replace_kernel(Args a)
 {
+    pdl_enter();
     State* st = a.st;
     if (st->done || !st->need_replace) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -385,6 +415,7 @@ __global__ void __launch_bounds__(kThreads, 3) mg_replace_kernel(Args a)
 template <class S, class T>
 __global__ void __launch_bounds__(kThreads, 3) mg_down_kernel(Args a, int l)
 {
+    pdl_enter();
     if (a.st->done) return;
     extern __shared__ __align__(16) unsigned char smem[];
     T* pt = reinterpret_cast<T*>(smem);
@@ -399,10 +430,7 @@ __global__ void __launch_bounds__(kThreads, 3) mg_down_kernel(Args a, int l)
         const int x0 = (t % tiles_x) * kTX, y0 = (t / tiles_x) * kDTY;
         __syncthreads();
         load_planes<T, S::NP, kDTY + kHalo>(pt, static_cast<const T*>(F.c), F.ps, P, W, H, x0, y0);
-        fill_tile<kDTY + 2 * kHalo>(vt, P, W, H, x0, y0, [&](size_t o, int, int) {
-            const float d = F.D[o];
-            return d > 0.f ? om * F.b[o] / d : 0.f;
-        });
+        fill_tile<kDTY + 2 * kHalo>(vt, P, W, H, x0, y0, [&](size_t o, int, int) { return om * F.b[o] * F.Di[o]; });
         __syncthreads();
         const int cx = (x0 >> 1) + tx, cy = (y0 >> 1) + ty;
         if (cx < C.W && cy < C.H) {
@@ -415,8 +443,7 @@ __global__ void __launch_bounds__(kThreads, 3) mg_down_kernel(Args a, int l)
                     const int gx = x0 + lx, gy = y0 + ly;
                     if (gx < W && gy < H) {
                         const size_t o = (size_t)gy * P + gx;
-                        const float Ax = sten_apply<S, T>(pt, kDTY + kHalo, vt, F.D[o], lx, ly);
-                        sum += F.b[o] - Ax;
+                        sum += rho_of(F.b[o], F.Di[o], om, sten_sum<S, T>(pt, kDTY + kHalo, vt, lx, ly));
                     }
                 }
             C.b[(size_t)cy * C.P + cx] = sum;
@@ -424,22 +451,148 @@ __global__ void __launch_bounds__(kThreads, 3) mg_down_kernel(Args a, int l)
     }
 }
 
-// Coarsest level: x = M^-1 b with the stored FP64 inverse (symmetric, read
-// by columns so consecutive threads read consecutive entries).
-__global__ void __launch_bounds__(kThreads) mg_coarse_kernel(Args a)
+// The small levels lt .. L of a V-cycle in ONE CTA: their operators and
+// vectors are staged in shared memory (compact [H_l][W_l] arrays) and the
+// phases (smoothing + restriction down to the coarsest level, the exact
+// coarsest solve with the stored FP64 inverse, prolongation + smoothing back
+// up) are separated by block barriers instead of kernel launches.  Reads
+// b_lt, writes x_lt.
+constexpr int kTailThreads = 1024;
+constexpr int kTailSmem = 160 * 1024;
+
+__device__ __forceinline__ float tail_sum(const float* c, const float* v, int W, int H, int n, int x, int y)
 {
-    if (a.st->done) return;
-    __shared__ double bs[kCoarseMax];
-    const Lev& C = a.lev[a.L];
-    const int n = C.W * C.H;
-    for (int i = threadIdx.x; i < n; i += kThreads) bs[i] = C.b[(size_t)(i / C.W) * C.P + i % C.W];
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += kThreads) {
-        double s = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < n; ++j) s += a.minv[(size_t)j * n + i] * bs[j];
-        C.x[(size_t)(i / C.W) * C.P + i % C.W] = (float)s;
+    const int i = y * W + x;
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int du = CoarseSten::du(k), dv = CoarseSten::dv(k);
+        const int xu = x + du, yu = y + dv, xl = x - du, yl = y - dv;
+        if (xu >= 0 && xu < W && yu < H) s = fmaf(c[k * n + i], v[yu * W + xu], s);
+        if (xl >= 0 && xl < W && yl >= 0) s = fmaf(c[k * n + yl * W + xl], v[yl * W + xl], s);
     }
+    return s;
+}
+
+__global__ void __launch_bounds__(kTailThreads) mg_tail_kernel(Args a)
+{
+    // The levels' operators and the coarsest inverse were written by the
+    // set-up kernels, which completed before this kernel's predecessor
+    // started (every other kernel waits before it triggers), so they are
+    // staged before the wait, overlapping the predecessor; b_lt after it.
+    pdl_trigger();
+    extern __shared__ __align__(16) float sh[];
+    const int lt = a.lt, L = a.L, tid = threadIdx.x;
+    const float om = a.omega, sc = a.scale;
+    // carve: per level c[4n], 1/D [n], b[n], x[n]; then tmp[n_lt]; then the
+    // coarsest inverse (FP64, rounded up to an 8-byte boundary)
+    auto base = [&](int l) {
+        int off = 0;
+        for (int m = lt; m < l; ++m) off += 7 * a.lev[m].W * a.lev[m].H;
+        return sh + off;
+    };
+    float* tmp = base(L + 1);
+    const int nL = a.lev[L].W * a.lev[L].H;
+    double* minv = reinterpret_cast<double*>(sh + ((int)(tmp - sh) + a.lev[lt].W * a.lev[lt].H + 1) / 2 * 2);
+    for (int l = lt; l <= L; ++l) {
+        const Lev& G = a.lev[l];
+        const int W = G.W, n = G.W * G.H;
+        float* c = base(l);
+        float* D = c + 4 * n;
+        const float* gc = static_cast<const float*>(G.c);
+        for (int i = tid; i < n; i += kTailThreads) {
+            const size_t g = (size_t)(i / W) * G.P + i % W;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) c[k * n + i] = gc[(size_t)k * G.ps + g];
+            D[i] = G.Di[g];
+        }
+    }
+    for (int i = tid; i < nL * nL; i += kTailThreads) minv[i] = a.minv[i];
+    pdl_wait();
+    if (a.st->done) return;
+    {
+        const Lev& G = a.lev[lt];
+        const int n = G.W * G.H;
+        float* b = base(lt) + 5 * n;
+        for (int i = tid; i < n; i += kTailThreads) b[i] = G.b[(size_t)(i / G.W) * G.P + i % G.W];
+    }
+    __syncthreads();
+    for (int l = lt; l < L; ++l) {
+        const Lev& F = a.lev[l];
+        const Lev& Cl = a.lev[l + 1];
+        const int W = F.W, H = F.H, n = W * H;
+        float* c = base(l);
+        float* D = c + 4 * n;
+        float* b = D + n;
+        float* x = b + n;
+        for (int i = tid; i < n; i += kTailThreads) x[i] = om * b[i] * D[i];
+        __syncthreads();
+        float* bc = base(l + 1) + 5 * Cl.W * Cl.H;
+        for (int I = tid; I < Cl.W * Cl.H; I += kTailThreads) {
+            const int X = I % Cl.W, Y = I / Cl.W;
+            float sum = 0.f;
+            for (int q = 0; q < 4; ++q) {
+                const int xf = 2 * X + (q & 1), yf = 2 * Y + (q >> 1);
+                if (xf < W && yf < H) {
+                    const int i = yf * W + xf;
+                    sum += rho_of(b[i], D[i], om, tail_sum(c, x, W, H, n, xf, yf));
+                }
+            }
+            bc[I] = sum;
+        }
+        __syncthreads();
+    }
+    {
+        const Lev& G = a.lev[L];
+        const int n = G.W * G.H;
+        float* b = base(L) + 5 * n;
+        float* x = b + n;
+        for (int i = tid; i < n; i += kTailThreads) {
+            double s = 0.0;
+#pragma unroll 8
+            for (int j = 0; j < n; ++j) s += minv[j * n + i] * (double)b[j];
+            x[i] = (float)s;
+        }
+        __syncthreads();
+    }
+    for (int l = L - 1; l >= lt; --l) {
+        const Lev& F = a.lev[l];
+        const Lev& Cl = a.lev[l + 1];
+        const int W = F.W, H = F.H, n = W * H;
+        float* c = base(l);
+        float* D = c + 4 * n;
+        float* b = D + n;
+        float* x = b + n;
+        const float* xc = base(l + 1) + 6 * Cl.W * Cl.H;
+        for (int i = tid; i < n; i += kTailThreads) {
+            const int xf = i % W, yf = i / W;
+            x[i] = fmaf(sc, xc[(yf >> 1) * Cl.W + (xf >> 1)], om * b[i] * D[i]);
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += kTailThreads) {
+            tmp[i] = smooth_of(x[i], b[i], D[i], om, tail_sum(c, x, W, H, n, i % W, i / W));
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += kTailThreads) x[i] = tmp[i];
+        __syncthreads();
+    }
+    {
+        const Lev& G = a.lev[lt];
+        const int n = G.W * G.H;
+        const float* x = base(lt) + 6 * n;
+        for (int i = tid; i < n; i += kTailThreads) G.x[(size_t)(i / G.W) * G.P + i % G.W] = x[i];
+    }
+}
+
+// Shared-memory bytes of the tail kernel for levels lt .. L.
+static int tail_bytes(const int* Wl, const int* Hl, int lt, int L)
+{
+    long long f = 0;
+    for (int l = lt; l <= L; ++l) f += 7LL * Wl[l] * Hl[l];
+    f += (long long)Wl[lt] * Hl[lt];
+    f = (f + 1) / 2 * 2;                        // the FP64 inverse starts 8-byte aligned
+    f += 2LL * Wl[L] * Hl[L] * Wl[L] * Hl[L];
+    return (int)(f * 4);
 }
 
 // Level l >= 1 from x_{l+1}: y = omega b / D + scale * x_{l+1}[aggregate]
@@ -447,6 +600,7 @@ __global__ void __launch_bounds__(kThreads) mg_coarse_kernel(Args a)
 template <class S, class T>
 __global__ void __launch_bounds__(kThreads, 3) mg_up_kernel(Args a, int l)
 {
+    pdl_enter();
     if (a.st->done) return;
     extern __shared__ __align__(16) unsigned char smem[];
     T* pt = reinterpret_cast<T*>(smem);
@@ -462,8 +616,7 @@ __global__ void __launch_bounds__(kThreads, 3) mg_up_kernel(Args a, int l)
         __syncthreads();
         load_planes<T, S::NP, kTY + kHalo>(pt, static_cast<const T*>(F.c), F.ps, P, W, H, x0, y0);
         fill_tile<kTY + 2 * kHalo>(vt, P, W, H, x0, y0, [&](size_t o, int gx, int gy) {
-            const float d = F.D[o];
-            return fmaf(sc, C.x[(size_t)(gy >> 1) * C.P + (gx >> 1)], d > 0.f ? om * F.b[o] / d : 0.f);
+            return fmaf(sc, C.x[(size_t)(gy >> 1) * C.P + (gx >> 1)], om * F.b[o] * F.Di[o]);
         });
         __syncthreads();
 #pragma unroll
@@ -471,10 +624,8 @@ __global__ void __launch_bounds__(kThreads, 3) mg_up_kernel(Args a, int l)
             const int lx = tx + 32 * h, gx = x0 + lx, gy = y0 + ty;
             if (gx < W && gy < H) {
                 const size_t o = (size_t)gy * P + gx;
-                const float d = F.D[o], bv = F.b[o];
-                const float Ay = sten_apply<S, T>(pt, kTY + kHalo, vt, d, lx, ty);
                 const float y = vt[(ty + kHalo) * kVW + lx + kHalo];
-                F.x[o] = d > 0.f ? fmaf(om, (bv - Ay) / d, y) : y;
+                F.x[o] = smooth_of(y, F.b[o], F.Di[o], om, sten_sum<S, T>(pt, kTY + kHalo, vt, lx, ty));
             }
         }
     }
@@ -515,6 +666,7 @@ __host__ __device__ constexpr int b128(int x) { return (x + 127) & ~127; }
 template <int MODE, int ES>
 struct FineLayout {
     static constexpr int TH = fine_rows(ES);
+    static constexpr int THR = ES == 2 ? 512 : 256;  // threads: 64 column pairs x TH / 2 row pairs
     static constexpr int PB = 12 * (TH + 2) * kFBW * ES;
     static constexpr int VB = (TH + 4) * kFBW * 4;
     static constexpr int XB = MODE == FM_UP ? (TH / 2 + 2) * kXBW * 4 : 0;
@@ -559,13 +711,16 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, State
 }
 
 template <int MODE, class T>
-__global__ void __launch_bounds__(kThreads, 1) mg_fine_kernel(const __grid_constant__ TMaps tm, Args a)
+__global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T)>::THR, 1)
+    mg_fine_kernel(const __grid_constant__ TMaps tm, Args a)
 {
     constexpr int ES = MODE == FM_SPMV ? 4 : (int)sizeof(T);
     using PT = typename std::conditional<MODE == FM_SPMV, float, T>::type;
     using LY = FineLayout<MODE, ES>;
-    constexpr int TH = LY::TH, RPT = TH / 4;
+    constexpr int TH = LY::TH, NT = LY::THR, RPT = TH / (NT / 64);
+    static_assert(RPT == 2, "each thread covers one row pair");
     constexpr int PW = (TH + 2) * kFBW;  // elements per plane in the box
+    pdl_enter();
     State* st = a.st;
     if (st->done) {
         if (MODE == FM_UP && blockIdx.x == 0 && threadIdx.x == 0) set_cond(a, 0u);
@@ -622,13 +777,12 @@ __global__ void __launch_bounds__(kThreads, 1) mg_fine_kernel(const __grid_const
         const float* v1b = reinterpret_cast<const float*>(sp + LY::v1_off);
         const int u0 = (t % ntx) * kFTW, v0 = (t / ntx) * TH;
         // stencil input tile
-        for (int i = tid; i < (TH + 4) * kFBW; i += kThreads) {
+        for (int i = tid; i < (TH + 4) * kFBW; i += NT) {
             float v;
             if (MODE == FM_SPMV) {
                 v = first ? v0b[i] : fmaf(beta, v1b[i], v0b[i]);
             } else {
-                const float d = v1b[i];
-                v = d > 0.f ? om * v0b[i] / d : 0.f;
+                v = om * v0b[i] * v1b[i];  // x1 = omega b / d (v1 holds 1 / d)
                 if (MODE == FM_UP) {
                     const int row = i / kFBW, col = i - row * kFBW;
                     const int gu = u0 - 8 + col, gv = v0 - 2 + row;
@@ -702,18 +856,18 @@ __global__ void __launch_bounds__(kThreads, 1) mg_fine_kernel(const __grid_const
                 }
             } else {
                 const float2 bb = *reinterpret_cast<const float2*>(v0b + (r + 2) * kFBW + lu);
-                const float2 dd = *reinterpret_cast<const float2*>(v1b + (r + 2) * kFBW + lu);
+                const float2 dd = *reinterpret_cast<const float2*>(v1b + (r + 2) * kFBW + lu);  // 1 / d
                 if (MODE == FM_DOWN) {
-                    // rho = b - A x1 = b - d x1 + S; zero outside the image (zero fill)
-                    cs += (bb.x - dd.x * xi0 + S0) + (bb.y - dd.y * xi1 + S1);
+                    // rho = b - A x1; zero outside the image (zero fill)
+                    cs += rho_of(bb.x, dd.x, om, S0) + rho_of(bb.y, dd.y, om, S1);
                     if (rr & 1) {
                         const int X = (u0 >> 1) + cp, Y = v >> 1;
                         if (X < C.W && Y < C.H) C.b[(size_t)Y * C.P + X] = cs;
                         cs = 0.f;
                     }
                 } else {
-                    const float z0 = dd.x > 0.f ? fmaf(om, (bb.x - fmaf(dd.x, xi0, -S0)) / dd.x, xi0) : xi0;
-                    const float z1 = dd.y > 0.f ? fmaf(om, (bb.y - fmaf(dd.y, xi1, -S1)) / dd.y, xi1) : xi1;
+                    const float z0 = smooth_of(xi0, bb.x, dd.x, om, S0);
+                    const float z1 = smooth_of(xi1, bb.y, dd.y, om, S1);
                     if (v < H) {
                         float* zr = a.lev[0].x + (size_t)v * P + u;
                         if (u + 1 < W) {
@@ -732,6 +886,7 @@ __global__ void __launch_bounds__(kThreads, 1) mg_fine_kernel(const __grid_const
         s ^= 1;
     }
     if (!ok) return;
+    static_assert(NT <= 1024, "");
     if (MODE == FM_SPMV) {
         double v[1] = {acc};
         if (last_cta_total<1>(v, a.parts, &st->ticket[T_PQ]) && threadIdx.x == 0) {
@@ -769,6 +924,7 @@ __global__ void __launch_bounds__(kThreads, 1) mg_fine_kernel(const __grid_const
 template <class S, class T>
 __global__ void mg_build_kernel(Args a, int l, const float* fine_gamma, int gpitch)
 {
+    pdl_enter();
     const Lev& F = a.lev[l];
     const Lev& C = a.lev[l + 1];
     const T* w = static_cast<const T*>(F.c);
@@ -802,6 +958,7 @@ __global__ void mg_build_kernel(Args a, int l, const float* fine_gamma, int gpit
         for (int o = 0; o < 4; ++o) cp[(size_t)o * C.ps + oc] = (float)c[o];
         C.gam[oc] = (float)gam;
         C.D[oc] = (float)(gam + ext);
+        C.Di[oc] = gam + ext > 0.0 ? (float)(1.0 / (gam + ext)) : 0.f;
     }
 }
 
@@ -809,6 +966,7 @@ __global__ void mg_build_kernel(Args a, int l, const float* fine_gamma, int gpit
 // elimination (SPD: no pivoting), one CTA, matrix in shared memory.
 __global__ void __launch_bounds__(kThreads) mg_inverse_kernel(Args a)
 {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem[];
     const Lev& C = a.lev[a.L];
     const int n = C.W * C.H;
@@ -882,9 +1040,23 @@ __global__ void __launch_bounds__(kThreads) mg_inverse_kernel(Args a)
     for (int e = threadIdx.x; e < n * n; e += kThreads) a.minv[e] = A[e];
 }
 
+// 1 / d of the level-0 iteration diagonal (0 where d = 0).
+__global__ void mg_diag0_kernel(Args a)
+{
+    pdl_enter();
+    const int W = a.W, H = a.H, P = a.P;
+    const size_t n = (size_t)W * H;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t o = (i / W) * P + i % W;
+        const float d = a.lev[0].D[o];
+        a.lev[0].Di[o] = d > 0.f ? 1.f / d : 0.f;
+    }
+}
+
 // Initial state, FP64 solution from the FP32 guess.
 __global__ void mg_init_kernel(Args a)
 {
+    pdl_enter();
     const int W = a.W, H = a.H, P = a.P;
     const size_t n = (size_t)W * H;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -906,6 +1078,7 @@ __global__ void mg_init_kernel(Args a)
 // Solution out (FP32), zero when b = 0.
 __global__ void mg_final_kernel(Args a)
 {
+    pdl_enter();
     const int W = a.W, H = a.H, P = a.P;
     const bool zero = !(a.st->bn2 > 0.0) && a.st->replacements > 0;
     const size_t n = (size_t)W * H;
@@ -925,7 +1098,7 @@ namespace gm {
 namespace mg {
 
 struct Plan {
-    int L;
+    int L, lt;
     int W[kMaxLevels], H[kMaxLevels];
 };
 
@@ -942,6 +1115,9 @@ static int make_plan(int W, int H, Plan& pl)
         if ((long long)w * h <= kCoarseMax) break;
     }
     pl.L = l;
+    // the tail takes the deepest levels that fit its shared memory
+    pl.lt = pl.L;
+    while (pl.lt > 1 && tail_bytes(pl.W, pl.H, pl.lt - 1, pl.L) <= kTailSmem) --pl.lt;
     return GM_OK;
 }
 
@@ -960,24 +1136,27 @@ static size_t carve(const Plan& pl, int P0, char* base, Args* a)
     float* p0 = (float*)take(n0 * 4);
     float* p1 = (float*)take(n0 * 4);
     float* z = (float*)take(n0 * 4);
+    float* di0 = (float*)take(n0 * 4);
     double* x = (double*)take(n0 * 8);
     if (a) {
         a->r = r; a->q = q; a->p0 = p0; a->p1 = p1; a->x = x;
         a->lev[0].b = r;
         a->lev[0].x = z;
+        a->lev[0].Di = di0;
     }
     for (int l = 1; l <= pl.L; ++l) {
         const int P = (pl.W[l] + 31) & ~31;
         const size_t n = (size_t)pl.H[l] * P;
         char* c = take(4 * n * 4);
         float* D = (float*)take(n * 4);
+        float* Di = (float*)take(n * 4);
         float* gam = (float*)take(n * 4);
         float* b = (float*)take(n * 4);
         float* xl = (float*)take(n * 4);
         if (a) {
             Lev& v = a->lev[l];
             v.W = pl.W[l]; v.H = pl.H[l]; v.P = P;
-            v.c = c; v.ps = n; v.D = D; v.gam = gam; v.b = b; v.x = xl;
+            v.c = c; v.ps = n; v.D = D; v.Di = Di; v.gam = gam; v.b = b; v.x = xl;
         }
     }
     double* minv = (double*)take((size_t)kCoarseMax * kCoarseMax * 8);
@@ -1058,7 +1237,17 @@ static int occupancy(const void* fn, int smem, int threads)
     cudaGetDevice(&dev);
     for (const E& e : cache)
         if (e.fn == fn && e.dev == dev && e.smem == smem) return e.occ;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (smem > 48 * 1024) {
+        // the largest size the kernel may ask for (opt-in maximum less its
+        // static shared memory), so graphs captured with other sizes stay valid
+        int optin = 0;
+        cudaFuncAttributes fa;
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, fn) == cudaSuccess)
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 std::max(smem, optin - (int)fa.sharedSizeBytes));
+        cudaGetLastError();
+    }
     int o = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, threads, smem) != cudaSuccess) o = 1;
     if (o < 1) o = 1;
@@ -1107,7 +1296,7 @@ static int make_maps(const Args& a, int es, CUtensorMapDataType dt, FineMaps& fm
     GM_TRY(vec(&fm.spmv.m[4], a.d32, W, H, P, kFTW, t32));
     GM_TRY(planes(&fm.down.m[0], L0.c, dt, (uint64_t)es, L0.ps, tlo));
     GM_TRY(vec(&fm.down.m[1], a.r, W, H, P, kFBW, tlo + 4));
-    GM_TRY(vec(&fm.down.m[2], L0.D, W, H, P, kFBW, tlo + 4));
+    GM_TRY(vec(&fm.down.m[2], L0.Di, W, H, P, kFBW, tlo + 4));
     fm.up = fm.down;
     GM_TRY(vec(&fm.up.m[3], L1.x, (uint64_t)L1.W, (uint64_t)L1.H, (uint64_t)L1.P, kXBW, tlo / 2 + 2));
     return GM_OK;
@@ -1125,7 +1314,18 @@ struct Enq {
     {
         int g = std::min(tiles, sms * occupancy((const void*)fn, smem, threads));
         g = std::max(1, std::min(g, kMaxParts));
-        if (!dry) fn<<<g, threads, smem, s>>>(args...);
+        if (dry) return;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)g);
+        cfg.blockDim = dim3((unsigned)threads);
+        cfg.dynamicSmemBytes = (size_t)smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, fn, args...);
     }
 
     int pointwise_tiles() const
@@ -1138,7 +1338,7 @@ struct Enq {
         using LY = FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T)>;
         const int tiles = ((a.W + kFTW - 1) / kFTW) * ((a.H + LY::TH - 1) / LY::TH);
         const TMaps& m = MODE == FM_SPMV ? fm->spmv : (MODE == FM_DOWN ? fm->down : fm->up);
-        go(mg_fine_kernel<MODE, T>, tiles, LY::total, kThreads, m, a);
+        go(mg_fine_kernel<MODE, T>, tiles, LY::total, LY::THR, m, a);
     }
 
     void down(int l) const
@@ -1165,9 +1365,11 @@ struct Enq {
 
     void vcycle() const
     {
-        for (int l = 0; l < a.L; ++l) down(l);
-        go(mg_coarse_kernel, 1, 0, kThreads, a);
-        for (int l = a.L - 1; l >= 0; --l) up(l);
+        for (int l = 0; l < a.lt; ++l) down(l);
+        int Wl[kMaxLevels], Hl[kMaxLevels];
+        for (int l = 0; l <= a.L; ++l) { Wl[l] = a.lev[l].W; Hl[l] = a.lev[l].H; }
+        go(mg_tail_kernel, 1, tail_bytes(Wl, Hl, a.lt, a.L), kTailThreads, a);
+        for (int l = a.lt - 1; l >= 0; --l) up(l);
     }
 
     void replace() const
@@ -1179,6 +1381,7 @@ struct Enq {
 
     void build() const
     {
+        go(mg_diag0_kernel, pointwise_tiles() * 4, 0, kThreads, a);
         for (int l = 0; l < a.L; ++l) {
             const Lev& C = a.lev[l + 1];
             const int t = (C.W * C.H + 127) / 128;
@@ -1292,6 +1495,7 @@ static int run(Dev& d, const Args& a0, const FineMaps& fm, int tcode, cudaStream
                 d.cond_ok = 1;
             } else if (d.cond_ok == -1) {
                 d.cond_ok = 0;  // conditional nodes unavailable: host-driven loop from now on
+                if (getenv("GM_MG_DEBUG")) fprintf(stderr, "gm_mg: graph path unavailable (%s)\n", gm_last_error());
             } else {
                 return rc;
             }
@@ -1344,6 +1548,7 @@ static int prepare(const gm_levin_store* store, int use_low, Plan& pl, Args& a, 
     }
     *tcode = low ? (store->precision == GM_PREC_FP16 ? 1 : 2) : 0;
     a.L = pl.L;
+    a.lt = pl.lt;
     a.W = W; a.H = H; a.P = P;
     Lev& f = a.lev[0];
     f.W = W; f.H = H; f.P = P;

@@ -53,7 +53,7 @@ def test_hierarchy_matches_oracle(orc, W, H, prec):
         assert np.allclose(D, ref.D, rtol=1e-5, atol=1e-6 * np.abs(ref.D).max()), level
 
 
-@pytest.mark.parametrize("prec", ["fp16", "fp32"])
+@pytest.mark.parametrize("prec", ["fp16", "bf16", "fp32"])
 def test_vcycle_matches_oracle(orc, prec):
     torch = torch_cuda()
     W, H = 200, 150
@@ -161,6 +161,58 @@ def test_mg_adjoint_matches_cg_adjoint(orc):
     for a_, b_ in ((lam_mg, lam_cg), (d_mg, d_cg), (dg_mg, dg_cg)):
         a_, b_ = a_.double().cpu().numpy(), b_.double().cpu().numpy()
         assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_)
+
+
+def test_mg_on_restricted_store_matches_fp64_elimination(orc):
+    """Hard constraints (gm_levin_restrict) then MG-PCG to 1e-10: within 1e-4
+    of the FP64 elimination of the known pixels."""
+    from tests.test_gpu_restrict import _reduced_solution
+
+    torch = torch_cuda()
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
+
+    W, H = 96, 64
+    p = make_problem(W, H, 8)
+    scr = torch.from_numpy(p.scribbles).cuda()
+    st = api.LevinStore(W, H, "fp16").assemble(torch.from_numpy(p.image).cuda(), scr, eps=p.eps).restrict(scribbles=scr)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    r = st.solve(alpha, "mg", rtol=1e-10, max_iters=5000)
+    assert r.status == 0 and r.rel_residual <= 1e-10, r
+    x, known, s = _reduced_solution(orc, p, W, H)
+    assert np.abs(alpha.double().cpu().numpy().ravel() - x).max() <= TOL
+
+
+def test_mg_on_batch_store_view(orc):
+    """A batch image's store view (planes inside the canvas, plane_stride set)
+    solves with MG like a standalone store of the same image."""
+    import ctypes as C
+
+    torch = torch_cuda()
+    from gpumatting_b200 import _lib as L
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
+
+    sizes = [(70, 41), (96, 64)]
+    b = api.LevinBatch(sizes, "fp16")
+    probs = [make_problem(w, h, k) for k, (w, h) in enumerate(sizes)]
+    for k, q in enumerate(probs):
+        b.assemble(k, torch.from_numpy(q.image).cuda(), torch.from_numpy(q.scribbles).cuda(), eps=q.eps)
+    W, H = sizes[1]
+    q = probs[1]
+    view = b.store_view(1)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    prm = L.default_params(solver=L.GM_SOLVER_MG, rtol=1e-8, max_iters=2000)
+    info = L.GmSolveInfo()
+    rc = L.load().gm_levin_solve(C.byref(view), alpha.data_ptr(), C.byref(prm), C.byref(info),
+                                 torch.cuda.current_stream().cuda_stream)
+    assert rc == 0 and info.rel_residual <= 1e-8, info.as_dict()
+    st = api.LevinStore(W, H, "fp16").assemble(torch.from_numpy(q.image).cuda(), torch.from_numpy(q.scribbles).cuda(),
+                                               eps=q.eps)
+    ref = torch.full((H, W), 0.5, device="cuda")
+    rs = st.solve(ref, "mg", rtol=1e-8, max_iters=2000)
+    assert rs.iters == info.iters
+    assert np.abs(alpha.cpu().numpy() - ref.cpu().numpy()).max() <= 1e-6
 
 
 def test_mg_rejected_where_unsupported(orc):

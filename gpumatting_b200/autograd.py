@@ -52,6 +52,7 @@ def levin_matte(image, gamma, s, eps: float = 1e-5, precision: str = "fp16", rto
                 max_iters: int = 5000, adjoint_rtol: float | None = None, solver: str = "cg"):
     """Differentiable matte: alpha (H, W) from image (H, W, 3) in [0, 1],
     per-pixel scribble weights gamma and targets s (both (H, W)).  solver:
-    "cg" or "pcg" (Jacobi-preconditioned) for both the solve and the adjoint."""
+    "cg", "pcg" (Jacobi-preconditioned) or "mg" (multigrid-preconditioned)
+    for both the solve and the adjoint."""
     return LevinMatte.apply(image, gamma, s, eps, precision, rtol, max_iters,
                             rtol if adjoint_rtol is None else adjoint_rtol, solver)

@@ -77,8 +77,10 @@ def test_adjoint_rgb8_layout_and_scribble_map(orc):
     assert _rel(dgamma.cpu().numpy(), ref["dgamma"]) <= 1e-3
 
 
-def test_autograd_512_matches_finite_differences():
-    """The torch.autograd path at 512x512 against the FP64 FD fixture."""
+@pytest.mark.parametrize("solver", ["cg", "mg"])
+def test_autograd_512_matches_finite_differences(solver):
+    """The torch.autograd path at 512x512 against the FP64 FD fixture, with
+    the fused CG and with the multigrid-preconditioned CG."""
     torch = torch_cuda()
     from gpumatting_b200.autograd import levin_matte
 
@@ -87,7 +89,8 @@ def test_autograd_512_matches_finite_differences():
     im, gamma, s, gt = _inputs(torch, p)
     im.requires_grad_(True)
     gamma.requires_grad_(True)
-    alpha = levin_matte(im, gamma, s, eps=float(g["eps"]), precision="fp16", rtol=1e-9, max_iters=20000)
+    alpha = levin_matte(im, gamma, s, eps=float(g["eps"]), precision="fp16", rtol=1e-9,
+                        max_iters=20000 if solver == "cg" else 3000, solver=solver)
     loss = torch.mean((alpha - gt) ** 2)
     loss.backward()
     assert abs(loss.item() - float(g["loss"])) <= 1e-4 * float(g["loss"])

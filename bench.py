@@ -674,6 +674,21 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
         if i >= 1:
             ms_pcg.append(e0.elapsed_time(e1))
     assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res_p), [r.status for r in res_p]
+    # multigrid PCG on the same store views: one graph launch per image, the
+    # images spread over up to 8 concurrent streams (gm_levin_solve_mg_many)
+    views = [batch.store_view(k) for k in range(len(sizes))]
+    ms_mg = []
+    for i in range(2 + args.batch_steps):
+        for a in alphas:
+            a.fill_(0.5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res_m = api.mg_solve_many(views, alphas, rtol=1e-6, max_iters=5000, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            ms_mg.append(e0.elapsed_time(e1))
+    assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in res_m), [r.status for r in res_m]
     its = [r.iters for r in res]
     batch_ms = allreduce_max(statistics.mean(ms), world)
     work = allreduce_sum(sum(W * H * i for (W, H), i in zip(sizes, its)), world)
@@ -685,7 +700,11 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
            "launch": "1 cooperative launch per GPU from a CUDA graph", "tuned_shape": shape, "tune_s": t_tune,
            "batch_pcg_ms": allreduce_max(statistics.mean(ms_pcg), world),
            "pcg_iters_min_mean_max": [min(r.iters for r in res_p), statistics.mean(r.iters for r in res_p),
-                                      max(r.iters for r in res_p)]}
+                                      max(r.iters for r in res_p)],
+           "batch_mg_ms": allreduce_max(statistics.mean(ms_mg), world),
+           "mg_iters_min_mean_max": [min(r.iters for r in res_m), statistics.mean(r.iters for r in res_m),
+                                     max(r.iters for r in res_m)],
+           "mg_launch": "1 graph launch per image on up to 8 concurrent streams"}
     if world > 1:
         return out
     # sequential plain FP32 solves of the same images
@@ -708,7 +727,8 @@ def run_batch(args, stream, world: int = 1, rank: int = 0) -> dict:
         del a, b, Lm, x
     out.update({"sequential_plain_fp32_ms": seq_ms, "sequential_iters_mean": statistics.mean(seq_its),
                 "speedup_vs_sequential_plain": seq_ms / batch_ms,
-                "pcg_speedup_vs_sequential_plain": seq_ms / out["batch_pcg_ms"]})
+                "pcg_speedup_vs_sequential_plain": seq_ms / out["batch_pcg_ms"],
+                "mg_speedup_vs_sequential_plain": seq_ms / out["batch_mg_ms"]})
     return out
 
 

@@ -133,6 +133,8 @@ SIGNATURES = {
     "gm_banded_solve": (_i, [BandedMatrix, _i, _vp, _i, _vp, C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo),
                              _vp]),
     "gm_levin_mg_levels": (_i, [_i, _i, C.POINTER(C.c_int), C.POINTER(C.c_int), _i]),
+    "gm_levin_solve_mg_many": (_i, [C.POINTER(C.POINTER(GmLevinStore)), C.POINTER(C.c_void_p), _i,
+                                    C.POINTER(GmSolveParams), C.POINTER(GmSolveInfo), _vp]),
     "gm_levin_mg_inspect": (_i, [C.POINTER(GmLevinStore), _i, _vp, _vp, _i, _vp, _vp, _vp]),
 }
 

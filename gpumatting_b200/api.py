@@ -456,6 +456,24 @@ def _wrap(ptr: int, shape, dtype):
     return torch.as_tensor(_CudaArray(ptr, shape, ts), device="cuda")
 
 
+def mg_solve_many(stores, alphas, stream=None, **params) -> list:
+    """gm_levin_solve_mg_many: independent multigrid solves, one graph launch
+    each, on up to 8 concurrent streams.  stores: LevinStore objects or
+    GmLevinStore structs (e.g. LevinBatch.store_view(k)); alphas: [H_k, W_k]
+    device float tensors (initial guess in, solution out)."""
+    n = len(stores)
+    assert len(alphas) == n
+    structs = [s.s if isinstance(s, LevinStore) else s for s in stores]
+    sp = (C.POINTER(L.GmLevinStore) * n)(*[C.pointer(x) for x in structs])
+    ap = (C.c_void_p * n)(*[a.data_ptr() for a in alphas])
+    infos = (L.GmSolveInfo * n)()
+    p = L.default_params(solver=L.GM_SOLVER_MG, **params)
+    rc = L.load().gm_levin_solve_mg_many(sp, ap, n, C.byref(p), infos, _stream(stream))
+    if rc not in (L.GM_OK, L.GM_ERR_NOT_CONVERGED):
+        L.check(rc)
+    return [SolveResult.from_info(infos[k]) for k in range(n)]
+
+
 def levin_bands25(image, scribbles=None, eps: float = 1e-5, gamma_value: float = 100.0, gamma_map=None, s_map=None,
                   arithmetic: str = "fp64", stream=None):
     """25-band FP32 reference-layout store (a (25, N), b (N,)) on the device."""

@@ -1166,8 +1166,10 @@ static size_t carve(const Plan& pl, int P0, char* base, Args* a)
     return off;
 }
 
-// Per-device resources: a grow-only workspace, a capture stream, pinned state
-// for the read-back, timing events and the cache of instantiated graphs.
+// Per-device solver slots: each has a grow-only workspace, capture streams,
+// an execution stream (for batches), pinned state for the read-back, timing
+// events and a cache of instantiated graphs.  Single solves use slot 0;
+// gm_levin_solve_mg_many spreads its images over the slots.
 struct Graph {
     Args key;
     int tcode;
@@ -1178,14 +1180,19 @@ struct Graph {
 struct Dev {
     void* ws = nullptr;
     size_t ws_bytes = 0;
-    cudaStream_t cap = nullptr, cap2 = nullptr;
+    cudaStream_t cap = nullptr, cap2 = nullptr, run = nullptr;
     State* host_state = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     std::vector<Graph> graphs;
     unsigned long long clock = 0;
     int sms = 0;
     int cond_ok = -1;  // conditional nodes usable (-1 unknown)
+    State* pin = nullptr;  // slot 0 only: pinned result states of a batch
+    int pin_n = 0;
 };
+
+constexpr int kSlots = 8;        // concurrent solves of gm_levin_solve_mg_many
+constexpr int kGraphCache = 16;  // instantiated graphs kept per slot
 
 // GM_MG_GRAPH=0 selects the host-driven loop (the same kernels launched
 // one by one, the done flag read every 4 iterations), e.g. for profilers
@@ -1197,7 +1204,7 @@ static bool graph_enabled()
 }
 
 static std::mutex g_mu;
-static Dev g_dev[64];
+static Dev g_dev[64][kSlots];
 
 static void drop_graphs(Dev& d)
 {
@@ -1210,9 +1217,11 @@ static int dev_setup(Dev& d, size_t bytes)
     if (!d.cap) {
         GM_CUDA_TRY(cudaStreamCreateWithFlags(&d.cap, cudaStreamNonBlocking));
         GM_CUDA_TRY(cudaStreamCreateWithFlags(&d.cap2, cudaStreamNonBlocking));
+        GM_CUDA_TRY(cudaStreamCreateWithFlags(&d.run, cudaStreamNonBlocking));
         GM_CUDA_TRY(cudaMallocHost((void**)&d.host_state, sizeof(State)));
         GM_CUDA_TRY(cudaEventCreate(&d.e0));
         GM_CUDA_TRY(cudaEventCreate(&d.e1));
+        GM_CUDA_TRY(cudaEventCreate(&d.e2));
     }
     if (d.ws_bytes < bytes) {
         drop_graphs(d);
@@ -1467,6 +1476,35 @@ static int build_graph(Dev& d, Args a, const FineMaps& fm, cudaGraphExec_t* exec
     return GM_OK;
 }
 
+// The cached graph of this solve on slot d, captured on first use.
+template <class T>
+static int graph_for(Dev& d, const Args& a, const FineMaps& fm, int tcode, Graph** out)
+{
+    *out = nullptr;
+    for (Graph& g : d.graphs)
+        if (g.tcode == tcode && memcmp(&g.key, &a, sizeof(Args)) == 0) *out = &g;
+    if (*out) {
+        (*out)->used = ++d.clock;
+        return GM_OK;
+    }
+    cudaGraphExec_t ex = nullptr;
+    GM_TRY(build_graph<T>(d, a, fm, &ex));
+    if (d.graphs.size() >= (size_t)kGraphCache) {
+        auto old = std::min_element(d.graphs.begin(), d.graphs.end(),
+                                    [](const Graph& x, const Graph& y) { return x.used < y.used; });
+        cudaGraphExecDestroy(old->exec);
+        d.graphs.erase(old);
+    }
+    Graph g;
+    memcpy(&g.key, &a, sizeof(Args));
+    g.tcode = tcode;
+    g.exec = ex;
+    g.used = ++d.clock;
+    d.graphs.push_back(g);
+    *out = &d.graphs.back();
+    return GM_OK;
+}
+
 template <class T>
 static int run(Dev& d, const Args& a0, const FineMaps& fm, int tcode, cudaStream_t st, float* ms)
 {
@@ -1479,7 +1517,7 @@ static int run(Dev& d, const Args& a0, const FineMaps& fm, int tcode, cudaStream
             cudaGraphExec_t ex = nullptr;
             const int rc = build_graph<T>(d, a, fm, &ex);
             if (rc == GM_OK) {
-                if (d.graphs.size() >= 8) {
+                if (d.graphs.size() >= (size_t)kGraphCache) {
                     auto old = std::min_element(d.graphs.begin(), d.graphs.end(),
                                                 [](const Graph& x, const Graph& y) { return x.used < y.used; });
                     cudaGraphExecDestroy(old->exec);
@@ -1528,6 +1566,54 @@ static int run(Dev& d, const Args& a0, const FineMaps& fm, int tcode, cudaStream
     GM_CUDA_TRY(cudaStreamSynchronize(st));
     GM_CUDA_TRY(cudaGetLastError());
     cudaEventElapsedTime(ms, d.e0, d.e1);
+    return GM_OK;
+}
+
+// One image of gm_levin_solve_mg_many.
+struct Item {
+    Plan pl;
+    Args a;
+    size_t bytes;
+    FineMaps fm;
+};
+
+// Launches every image's graph on the execution stream of its slot (image k
+// on slot k mod K), forked from and joined back to st, and copies each
+// image's final state to pinned memory on the same stream.  The images of one
+// slot run one after another (they share its workspace); different slots run
+// concurrently.  One host synchronisation for the whole batch.
+template <class T>
+static int run_many(Dev* slots, int K, std::vector<Item>& items, int tcode, cudaStream_t st, float* ms)
+{
+    const int n = (int)items.size();
+    Dev& d0 = slots[0];
+    std::vector<cudaGraphExec_t> ex(n);
+    for (int k = 0; k < n; ++k) {
+        Graph* g = nullptr;
+        GM_TRY(graph_for<T>(slots[k % K], items[k].a, items[k].fm, tcode, &g));
+        ex[k] = g->exec;
+    }
+    if (d0.pin_n < n) {
+        if (d0.pin) cudaFreeHost(d0.pin);
+        d0.pin = nullptr;
+        d0.pin_n = 0;
+        GM_CUDA_TRY(cudaMallocHost((void**)&d0.pin, (size_t)n * sizeof(State)));
+        d0.pin_n = n;
+    }
+    GM_CUDA_TRY(cudaEventRecord(d0.e0, st));
+    for (int j = 0; j < K; ++j) GM_CUDA_TRY(cudaStreamWaitEvent(slots[j].run, d0.e0, 0));
+    for (int k = 0; k < n; ++k) {
+        Dev& d = slots[k % K];
+        GM_CUDA_TRY(cudaGraphLaunch(ex[k], d.run));
+        GM_CUDA_TRY(cudaMemcpyAsync(d0.pin + k, items[k].a.st, sizeof(State), cudaMemcpyDeviceToHost, d.run));
+    }
+    for (int j = 0; j < K; ++j) {
+        GM_CUDA_TRY(cudaEventRecord(slots[j].e1, slots[j].run));
+        GM_CUDA_TRY(cudaStreamWaitEvent(st, slots[j].e1, 0));
+    }
+    GM_CUDA_TRY(cudaEventRecord(d0.e2, st));
+    GM_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(ms, d0.e0, d0.e2);
     return GM_OK;
 }
 
@@ -1594,7 +1680,7 @@ int run_mg_solver(const gm_levin_store* store, const float* b, int bpitch, const
     int dev = 0;
     GM_TRY(dev_index(&dev));
     std::lock_guard<std::mutex> g(g_mu);
-    Dev& d = g_dev[dev];
+    Dev& d = g_dev[dev][0];
     d.sms = sms;
     GM_TRY(dev_setup(d, bytes));
     carve(pl, a.P, (char*)d.ws, &a);
@@ -1635,7 +1721,107 @@ int run_mg_solver(const gm_levin_store* store, const float* b, int bpitch, const
     return s.status;
 }
 
+static void fill_info(gm_solve_info* info, const mg::State& s, float ms, int levels)
+{
+    memset(info, 0, sizeof(*info));
+    info->status = s.status;
+    info->iters = s.iter;
+    info->replacements = s.replacements;
+    info->bnorm = std::sqrt(s.bn2);
+    info->rel_residual = s.bn2 > 0.0 ? std::sqrt(s.rr_true / s.bn2) : 0.0;
+    info->kernel_ms = ms;
+    info->grid = levels;
+    info->where = 0;
+}
+
 }  // namespace gm
+
+// Many independent multigrid solves at once (see gpumat.h).
+extern "C" int gm_levin_solve_mg_many(const gm_levin_store* const* stores, float* const* alphas, int count,
+                                      const gm_solve_params* prm, gm_solve_info* infos, void* stream)
+{
+    using namespace gm;
+    using namespace gm::mg;
+    gm_solve_params p;
+    if (prm) p = *prm; else gm_default_params(&p);
+    if (count < 0 || (count > 0 && (!stores || !alphas))) {
+        gm_set_error_msg("gm_levin_solve_mg_many: bad arguments");
+        return GM_ERR_INVALID;
+    }
+    if (count == 0) return GM_OK;
+    if (p.max_iters < 0) { gm_set_error_msg("max_iters must be >= 0"); return GM_ERR_INVALID; }
+    int sms = 0;
+    GM_TRY(gm_check_device(&sms));
+    std::vector<Item> items((size_t)count);
+    int tcode = -1;
+    for (int k = 0; k < count; ++k) {
+        if (!stores[k] || !stores[k]->w32 || !alphas[k]) {
+            gm_set_error_msg("gm_levin_solve_mg_many: image %d has no store or alpha", k);
+            return GM_ERR_INVALID;
+        }
+        int tc = 0;
+        GM_TRY(prepare(stores[k], p.use_low, items[k].pl, items[k].a, &items[k].bytes, &tc));
+        if (tcode >= 0 && tc != tcode) {
+            gm_set_error_msg("gm_levin_solve_mg_many: all stores must have the same precision");
+            return GM_ERR_INVALID;
+        }
+        tcode = tc;
+    }
+    int dev = 0;
+    GM_TRY(dev_index(&dev));
+    std::lock_guard<std::mutex> g(g_mu);
+    Dev* slots = g_dev[dev];
+    const bool graphs = graph_enabled() && slots[0].cond_ok != 0;
+    const int K = graphs ? std::min(kSlots, count) : 1;
+    for (int j = 0; j < K; ++j) {
+        size_t need = 0;
+        for (int k = j; k < count; k += K) need = std::max(need, items[k].bytes);
+        slots[j].sms = sms;
+        GM_TRY(dev_setup(slots[j], need));
+    }
+    for (int k = 0; k < count; ++k) {
+        Args& a = items[k].a;
+        carve(items[k].pl, a.P, (char*)slots[k % K].ws, &a);
+        a.bvec = stores[k]->b;
+        a.bpitch = stores[k]->pitch;
+        a.alpha_in = alphas[k];
+        a.alpha_out = alphas[k];
+        a.rtol = p.rtol;
+        a.max_iters = p.max_iters;
+        a.replace_every = p.replace_every;
+        a.omega = p.mg_omega > 0.f ? p.mg_omega : 0.8f;
+        a.scale = p.mg_scale > 0.f ? p.mg_scale : 1.8f;
+        GM_TRY(make_maps(a, tcode ? 2 : 4, tcode_dtype(tcode), items[k].fm));
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int worst = GM_OK;
+    if (!graphs) {
+        // no conditional graphs here: one solve after another on slot 0
+        for (int k = 0; k < count; ++k) {
+            float ms = 0.f;
+            int rc;
+            if (tcode == 1) rc = run<__half>(slots[0], items[k].a, items[k].fm, tcode, st, &ms);
+            else if (tcode == 2) rc = run<__nv_bfloat16>(slots[0], items[k].a, items[k].fm, tcode, st, &ms);
+            else rc = run<float>(slots[0], items[k].a, items[k].fm, tcode, st, &ms);
+            if (rc != GM_OK) return rc;
+            if (infos) fill_info(&infos[k], *slots[0].host_state, ms, items[k].pl.L + 1);
+            worst = std::max(worst, slots[0].host_state->status);
+        }
+    } else {
+        float ms = 0.f;
+        int rc;
+        if (tcode == 1) rc = run_many<__half>(slots, K, items, tcode, st, &ms);
+        else if (tcode == 2) rc = run_many<__nv_bfloat16>(slots, K, items, tcode, st, &ms);
+        else rc = run_many<float>(slots, K, items, tcode, st, &ms);
+        if (rc != GM_OK) return rc;
+        for (int k = 0; k < count; ++k) {
+            if (infos) fill_info(&infos[k], slots[0].pin[k], ms, items[k].pl.L + 1);
+            worst = std::max(worst, slots[0].pin[k].status);
+        }
+    }
+    if (worst != GM_OK) gm_set_error_msg("multigrid batch: an image ended with status %d", worst);
+    return worst;
+}
 
 // ---------------------------------------------------------------------------
 // C ABI: level shapes and an inspection entry for tests
@@ -1669,7 +1855,7 @@ extern "C" int gm_levin_mg_inspect(const gm_levin_store* store, int use_low, con
     int dev = 0;
     GM_TRY(dev_index(&dev));
     std::lock_guard<std::mutex> g(g_mu);
-    Dev& d = g_dev[dev];
+    Dev& d = g_dev[dev][0];
     d.sms = sms;
     GM_TRY(dev_setup(d, bytes));
     carve(pl, a.P, (char*)d.ws, &a);

@@ -312,6 +312,19 @@ int gm_levin_adjoint(const gm_levin_store* st, const gm_image* im, const gm_scri
                      size_t dimage_pitch, int dimage_channels, float* dgamma, const gm_solve_params* p,
                      gm_solve_info* info, void* stream);
 
+/* Solves `count` independent assembled stores with GM_SOLVER_MG (p->solver
+ * is ignored), each with its own right-hand side st->b, alpha k in/out
+ * ([H_k][W_k] device floats, initial guess in).  The solves run as one graph
+ * launch each, spread over up to 8 concurrent streams forked from `stream`
+ * and joined back to it, with one host synchronisation for the whole set
+ * (small images do not fill the GPU alone).  All stores must have the same
+ * precision.  infos: `count` results (kernel_ms is the whole set's time).
+ * Returns the largest per-image status.  No counterpart in the reference,
+ * which solves one image per process (main.cu:106-316); the batched solver
+ * (gm_batch_solve) runs CG / PCG in one persistent launch instead. */
+int gm_levin_solve_mg_many(const gm_levin_store* const* stores, float* const* alphas, int count,
+                           const gm_solve_params* p, gm_solve_info* infos, void* stream);
+
 /* Level shapes of the GM_SOLVER_MG hierarchy for a W x H image: *nlevels
  * levels, dims[2l], dims[2l+1] = width, height of level l (up to cap). */
 int gm_levin_mg_levels(int W, int H, int* nlevels, int* dims, int cap);

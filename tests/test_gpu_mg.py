@@ -215,6 +215,35 @@ def test_mg_on_batch_store_view(orc):
     assert np.abs(alpha.cpu().numpy() - ref.cpu().numpy()).max() <= 1e-6
 
 
+def test_mg_many_matches_single_solves(orc):
+    """gm_levin_solve_mg_many (images spread over concurrent streams) gives
+    each image the same result as its own solve, call after call."""
+    torch = torch_cuda()
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
+
+    sizes = [(96, 64), (70, 41), (160, 120), (37, 29), (200, 150), (64, 48), (33, 90), (128, 128), (50, 40),
+             (75, 20)]
+    stores, probs = [], []
+    for k, (w, h) in enumerate(sizes):
+        q = make_problem(w, h, 20 + k)
+        probs.append(q)
+        stores.append(api.LevinStore(w, h, "fp16").assemble(torch.from_numpy(q.image).cuda(),
+                                                            torch.from_numpy(q.scribbles).cuda(), eps=q.eps))
+    refs = []
+    for st, (w, h) in zip(stores, sizes):
+        a = torch.full((h, w), 0.5, device="cuda")
+        r = st.solve(a, "mg", rtol=1e-6, max_iters=2000)
+        assert r.status == 0, r
+        refs.append((a.cpu().numpy(), r.iters))
+    for rep in range(2):
+        alphas = [torch.full((h, w), 0.5, device="cuda") for w, h in sizes]
+        res = api.mg_solve_many(stores, alphas, rtol=1e-6, max_iters=2000)
+        for r, a, (ref, it) in zip(res, alphas, refs):
+            assert r.status == 0 and r.rel_residual <= 1e-6 and r.iters == it, r
+            assert np.array_equal(a.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
 def test_mg_rejected_where_unsupported(orc):
     torch = torch_cuda()
     from gpumatting_b200 import _lib as L

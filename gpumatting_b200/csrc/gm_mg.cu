@@ -1575,10 +1575,11 @@ struct Item {
     Args a;
     size_t bytes;
     FineMaps fm;
+    int slot;
 };
 
-// Launches every image's graph on the execution stream of its slot (image k
-// on slot k mod K), forked from and joined back to st, and copies each
+// Launches every image's graph on the execution stream of its slot, forked
+// from and joined back to st, and copies each
 // image's final state to pinned memory on the same stream.  The images of one
 // slot run one after another (they share its workspace); different slots run
 // concurrently.  One host synchronisation for the whole batch.
@@ -1590,7 +1591,7 @@ static int run_many(Dev* slots, int K, std::vector<Item>& items, int tcode, cuda
     std::vector<cudaGraphExec_t> ex(n);
     for (int k = 0; k < n; ++k) {
         Graph* g = nullptr;
-        GM_TRY(graph_for<T>(slots[k % K], items[k].a, items[k].fm, tcode, &g));
+        GM_TRY(graph_for<T>(slots[items[k].slot], items[k].a, items[k].fm, tcode, &g));
         ex[k] = g->exec;
     }
     if (d0.pin_n < n) {
@@ -1603,7 +1604,7 @@ static int run_many(Dev* slots, int K, std::vector<Item>& items, int tcode, cuda
     GM_CUDA_TRY(cudaEventRecord(d0.e0, st));
     for (int j = 0; j < K; ++j) GM_CUDA_TRY(cudaStreamWaitEvent(slots[j].run, d0.e0, 0));
     for (int k = 0; k < n; ++k) {
-        Dev& d = slots[k % K];
+        Dev& d = slots[items[k].slot];
         GM_CUDA_TRY(cudaGraphLaunch(ex[k], d.run));
         GM_CUDA_TRY(cudaMemcpyAsync(d0.pin + k, items[k].a.st, sizeof(State), cudaMemcpyDeviceToHost, d.run));
     }
@@ -1773,15 +1774,31 @@ extern "C" int gm_levin_solve_mg_many(const gm_levin_store* const* stores, float
     Dev* slots = g_dev[dev];
     const bool graphs = graph_enabled() && slots[0].cond_ok != 0;
     const int K = graphs ? std::min(kSlots, count) : 1;
+    // Deal the images to the slots largest first, each to the least-loaded
+    // slot (a fixed per-solve cost plus the pixels); the deal depends only
+    // on the shapes, so repeated calls reuse each slot's cached graphs.
+    {
+        std::vector<int> order(count);
+        for (int k = 0; k < count; ++k) order[k] = k;
+        auto cost = [&](int k) { return (double)items[k].a.W * items[k].a.H + 2.0e5; };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+        std::vector<double> load(K, 0.0);
+        for (int k : order) {
+            const int j = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            items[k].slot = j;
+            load[j] += cost(k);
+        }
+    }
     for (int j = 0; j < K; ++j) {
         size_t need = 0;
-        for (int k = j; k < count; k += K) need = std::max(need, items[k].bytes);
+        for (int k = 0; k < count; ++k)
+            if (items[k].slot == j) need = std::max(need, items[k].bytes);
         slots[j].sms = sms;
         GM_TRY(dev_setup(slots[j], need));
     }
     for (int k = 0; k < count; ++k) {
         Args& a = items[k].a;
-        carve(items[k].pl, a.P, (char*)slots[k % K].ws, &a);
+        carve(items[k].pl, a.P, (char*)slots[items[k].slot].ws, &a);
         a.bvec = stores[k]->b;
         a.bpitch = stores[k]->pitch;
         a.alpha_in = alphas[k];

@@ -259,7 +259,7 @@ typedef struct gm_solve_params_s {
                              waits for one arrival that never comes, so the call
                              must end with GM_ERR_TIMEOUT after timeout_s */
     float mg_omega;       /* GM_SOLVER_MG: smoother damping (0 = 0.8)      */
-    float mg_scale;       /* GM_SOLVER_MG: coarse-correction scale (0 = 1.8) */
+    float mg_scale;       /* GM_SOLVER_MG: coarse-correction scale (0 = 1.5) */
 } gm_solve_params;
 
 typedef struct gm_solve_info_s {

@@ -35,7 +35,7 @@ import numpy as np
 
 COARSE_MAX = 128
 OMEGA = 0.8
-SCALE = 1.8
+SCALE = 1.5
 # upper offsets of the coarse 9-point stencil, in plane order
 COARSE_OFFS = ((1, 0), (-1, 1), (0, 1), (1, 1))
 

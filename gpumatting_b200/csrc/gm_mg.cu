@@ -1835,7 +1835,29 @@ extern "C" int gm_levin_solve_mg_many(const gm_levin_store* const* stores, float
         if (tcode == 1) rc = run_many<__half>(slots, K, items, tcode, st, &ms);
         else if (tcode == 2) rc = run_many<__nv_bfloat16>(slots, K, items, tcode, st, &ms);
         else rc = run_many<float>(slots, K, items, tcode, st, &ms);
+        if (rc != GM_OK && slots[0].cond_ok == -1) {
+            // the first capture failed: no conditional graphs here, so solve
+            // the images one after another with the host-driven loop
+            slots[0].cond_ok = 0;
+            if (getenv("GM_MG_DEBUG")) fprintf(stderr, "gm_mg: graph path unavailable (%s)\n", gm_last_error());
+            for (int k = 0; k < count; ++k) {
+                GM_TRY(dev_setup(slots[0], items[k].bytes));
+                Args& a = items[k].a;
+                carve(items[k].pl, a.P, (char*)slots[0].ws, &a);
+                GM_TRY(make_maps(a, tcode ? 2 : 4, tcode_dtype(tcode), items[k].fm));
+                float ms1 = 0.f;
+                if (tcode == 1) rc = run<__half>(slots[0], a, items[k].fm, tcode, st, &ms1);
+                else if (tcode == 2) rc = run<__nv_bfloat16>(slots[0], a, items[k].fm, tcode, st, &ms1);
+                else rc = run<float>(slots[0], a, items[k].fm, tcode, st, &ms1);
+                if (rc != GM_OK) return rc;
+                if (infos) fill_info(&infos[k], *slots[0].host_state, ms1, items[k].pl.L + 1);
+                worst = std::max(worst, slots[0].host_state->status);
+            }
+            if (worst != GM_OK) gm_set_error_msg("multigrid batch: an image ended with status %d", worst);
+            return worst;
+        }
         if (rc != GM_OK) return rc;
+        slots[0].cond_ok = 1;
         for (int k = 0; k < count; ++k) {
             if (infos) fill_info(&infos[k], slots[0].pin[k], ms, items[k].pl.L + 1);
             worst = std::max(worst, slots[0].pin[k].status);

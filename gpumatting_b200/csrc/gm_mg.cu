@@ -668,11 +668,11 @@ struct TMaps {
 __host__ __device__ constexpr int fine_rows(int esize) { return esize == 2 ? 16 : 8; }
 __host__ __device__ constexpr int b128(int x) { return (x + 127) & ~127; }
 
-template <int MODE, int ES>
+template <int MODE, int ES, int NP = 12>
 struct FineLayout {
     static constexpr int TH = fine_rows(ES);
     static constexpr int THR = ES == 2 ? 512 : 256;  // threads: 64 column pairs x TH / 2 row pairs
-    static constexpr int PB = 12 * (TH + 2) * kFBW * ES;
+    static constexpr int PB = NP * (TH + 2) * kFBW * ES;
     static constexpr int VB = (TH + 4) * kFBW * 4;
     static constexpr int XB = MODE == FM_UP ? (TH / 2 + 2) * kXBW * 4 : 0;
     static constexpr int DB = MODE == FM_SPMV ? TH * kFTW * 4 : 0;
@@ -715,13 +715,13 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, State
     return true;
 }
 
-template <int MODE, class T>
-__global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T)>::THR, 1)
-    mg_fine_kernel(const __grid_constant__ TMaps tm, Args a)
+template <int MODE, class S, class T>
+__global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T), S::NP>::THR, 1)
+    mg_fine_kernel(const __grid_constant__ TMaps tm, Args a, int l)
 {
     constexpr int ES = MODE == FM_SPMV ? 4 : (int)sizeof(T);
     using PT = typename std::conditional<MODE == FM_SPMV, float, T>::type;
-    using LY = FineLayout<MODE, ES>;
+    using LY = FineLayout<MODE, ES, S::NP>;
     constexpr int TH = LY::TH, NT = LY::THR, RPT = TH / (NT / 64);
     static_assert(RPT == 2, "each thread covers one row pair");
     constexpr int PW = (TH + 2) * kFBW;  // elements per plane in the box
@@ -737,14 +737,15 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
     unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + LY::bar_off);
     float* vt = reinterpret_cast<float*>(smem + LY::vt_off);
-    const int W = a.W, H = a.H, P = a.P, tid = threadIdx.x, G = gridDim.x;
+    const Lev& F = a.lev[l];
+    const int W = F.W, H = F.H, P = F.P, tid = threadIdx.x, G = gridDim.x;
     const int ntx = (W + kFTW - 1) / kFTW, ntiles = ntx * ((H + TH - 1) / TH);
     const int it = st->iter;
     const bool first = it == 0;
     const float beta = (float)st->beta, om = a.omega, sc = a.scale;
     const CUtensorMap* mv1 = MODE == FM_SPMV ? ((it & 1) ? &tm.m[3] : &tm.m[2]) : &tm.m[2];
     float* pnew = (it & 1) ? a.p0 : a.p1;
-    const Lev& C = a.lev[1];
+    const Lev& C = a.lev[l + 1];
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -831,9 +832,9 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
             // S = sum_j w_ij x_j, two chains per pixel
             float a0[2] = {0.f, 0.f}, a1[2] = {0.f, 0.f};
 #pragma unroll
-            for (int k = 1; k <= 12; ++k) {
-                const int dv = (k + 2) / 5, du = k - 5 * dv;
-                const PT* pk = wb + (k - 1) * PW;
+            for (int k = 0; k < S::NP; ++k) {
+                const int dv = S::dv(k), du = S::du(k);
+                const PT* pk = wb + k * PW;
                 const float2 wo = ld2<PT>(pk + (r + 2) * kFBW + lu);
                 const PT* pm = pk + (r + 2 - dv) * kFBW + lu - du;
                 const float wm0 = tof(pm[0]), wm1 = tof(pm[1]);
@@ -874,7 +875,7 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
                     const float z0 = smooth_of(xi0, bb.x, dd.x, om, S0);
                     const float z1 = smooth_of(xi1, bb.y, dd.y, om, S1);
                     if (v < H) {
-                        float* zr = a.lev[0].x + (size_t)v * P + u;
+                        float* zr = F.x + (size_t)v * P + u;
                         if (u + 1 < W) {
                             *reinterpret_cast<float2*>(zr) = make_float2(z0, z1);
                             acc += (double)bb.x * z0 + (double)bb.y * z1;
@@ -903,7 +904,7 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
                 st->alpha = st->rz / v[0];
             }
         }
-    } else if (MODE == FM_UP) {
+    } else if (MODE == FM_UP && l == 0) {
         double v[1] = {acc};
         if (last_cta_total<1>(v, a.parts + 4 * kMaxParts, &st->ticket[T_RZ]) && threadIdx.x == 0) {
             const double rz = v[0];
@@ -1279,8 +1280,10 @@ static int tiles_of(int W, int H, int ty) { return ((W + kTX - 1) / kTX) * ((H +
 // Enqueues kernels on one stream.  The template argument is the element type
 // of the fine iteration planes.  A dry pass only computes the launch shapes
 // (it sets the kernels' shared-memory limits before any stream capture).
+// Tensor maps of the TMA-pipelined kernels: the level-0 SpMV, and the
+// restriction / prolongation of every level below the tail.
 struct FineMaps {
-    TMaps spmv, down, up;
+    TMaps spmv, down[kMaxLevels], up[kMaxLevels];
 };
 
 // Tensor maps of the level-0 kernels (es: bytes per element of the
@@ -1302,17 +1305,28 @@ static int make_maps(const Args& a, int es, CUtensorMapDataType dt, FineMaps& fm
     };
     const int t32 = fine_rows(4), tlo = fine_rows(es);
     const Lev& L0 = a.lev[0];
-    const Lev& L1 = a.lev[1];
     GM_TRY(planes(&fm.spmv.m[0], a.w32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.ps32, t32));
     GM_TRY(vec(&fm.spmv.m[1], L0.x, W, H, P, kFBW, t32 + 4));
     GM_TRY(vec(&fm.spmv.m[2], a.p0, W, H, P, kFBW, t32 + 4));
     GM_TRY(vec(&fm.spmv.m[3], a.p1, W, H, P, kFBW, t32 + 4));
     GM_TRY(vec(&fm.spmv.m[4], a.d32, W, H, P, kFTW, t32));
-    GM_TRY(planes(&fm.down.m[0], L0.c, dt, (uint64_t)es, L0.ps, tlo));
-    GM_TRY(vec(&fm.down.m[1], a.r, W, H, P, kFBW, tlo + 4));
-    GM_TRY(vec(&fm.down.m[2], L0.Di, W, H, P, kFBW, tlo + 4));
-    fm.up = fm.down;
-    GM_TRY(vec(&fm.up.m[3], L1.x, (uint64_t)L1.W, (uint64_t)L1.H, (uint64_t)L1.P, kXBW, tlo / 2 + 2));
+    for (int l = 0; l < a.lt; ++l) {
+        // level 0: the store's planes (12, iteration precision); below: 4 FP32 planes
+        const Lev& F = a.lev[l];
+        const Lev& Cl = a.lev[l + 1];
+        const int np = l == 0 ? 12 : 4;
+        const uint64_t e = l == 0 ? (uint64_t)es : 4;
+        const int th = l == 0 ? tlo : t32;
+        const uint64_t Wl = (uint64_t)F.W, Hl = (uint64_t)F.H, Pl = (uint64_t)F.P;
+        const uint64_t d3[3] = {Wl, Hl, (uint64_t)np};
+        const uint64_t s3[2] = {Pl * e, (uint64_t)F.ps * e};
+        const uint32_t b3[3] = {(uint32_t)kFBW, (uint32_t)(th + 2), (uint32_t)np};
+        GM_TRY(gm_make_tmap(&fm.down[l].m[0], l == 0 ? dt : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, F.c, d3, s3, b3));
+        GM_TRY(vec(&fm.down[l].m[1], F.b, Wl, Hl, Pl, kFBW, th + 4));
+        GM_TRY(vec(&fm.down[l].m[2], F.Di, Wl, Hl, Pl, kFBW, th + 4));
+        fm.up[l] = fm.down[l];
+        GM_TRY(vec(&fm.up[l].m[3], Cl.x, (uint64_t)Cl.W, (uint64_t)Cl.H, (uint64_t)Cl.P, kXBW, th / 2 + 2));
+    }
     return GM_OK;
 }
 
@@ -1347,35 +1361,25 @@ struct Enq {
         return (int)std::min<size_t>((size_t)sms * 4, ((size_t)(a.W + 3) / 4 * a.H + kThreads - 1) / kThreads);
     }
 
-    template <int MODE> void fine() const
-    {
-        using LY = FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T)>;
-        const int tiles = ((a.W + kFTW - 1) / kFTW) * ((a.H + LY::TH - 1) / LY::TH);
-        const TMaps& m = MODE == FM_SPMV ? fm->spmv : (MODE == FM_DOWN ? fm->down : fm->up);
-        go(mg_fine_kernel<MODE, T>, tiles, LY::total, LY::THR, m, a);
-    }
-
-    void down(int l) const
+    // The TMA-pipelined kernels: level 0 with the store's 12 planes in the
+    // iteration precision, the levels below with their 4 FP32 planes.
+    template <int MODE> void fine(int l) const
     {
         const Lev& F = a.lev[l];
+        const TMaps& m = MODE == FM_SPMV ? fm->spmv : (MODE == FM_DOWN ? fm->down[l] : fm->up[l]);
         if (l == 0) {
-            fine<FM_DOWN>();
+            using LY = FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T), 12>;
+            const int tiles = ((F.W + kFTW - 1) / kFTW) * ((F.H + LY::TH - 1) / LY::TH);
+            go(mg_fine_kernel<MODE, FineSten, T>, tiles, LY::total, LY::THR, m, a, 0);
         } else {
-            constexpr int sm = tile_smem<float, CoarseSten>(kDTY + kHalo, kDTY + 2 * kHalo);
-            go(mg_down_kernel<CoarseSten, float>, tiles_of(F.W, F.H, kDTY), sm, kThreads, a, l);
+            using LY = FineLayout<MODE, 4, 4>;
+            const int tiles = ((F.W + kFTW - 1) / kFTW) * ((F.H + LY::TH - 1) / LY::TH);
+            go(mg_fine_kernel<MODE, CoarseSten, float>, tiles, LY::total, LY::THR, m, a, l);
         }
     }
 
-    void up(int l) const
-    {
-        const Lev& F = a.lev[l];
-        if (l == 0) {
-            fine<FM_UP>();
-        } else {
-            constexpr int sm = tile_smem<float, CoarseSten>(kTY + kHalo, kTY + 2 * kHalo);
-            go(mg_up_kernel<CoarseSten, float>, tiles_of(F.W, F.H, kTY), sm, kThreads, a, l);
-        }
-    }
+    void down(int l) const { fine<FM_DOWN>(l); }
+    void up(int l) const { fine<FM_UP>(l); }
 
     void vcycle() const
     {
@@ -1417,7 +1421,7 @@ struct Enq {
 
     void iteration() const
     {
-        fine<FM_SPMV>();
+        fine<FM_SPMV>(0);
         go(mg_update_kernel, pointwise_tiles(), 0, kThreads, a);
         replace();
         vcycle();

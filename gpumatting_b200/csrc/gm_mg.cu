@@ -55,7 +55,6 @@ constexpr int kMaxLevels = 24;
 constexpr int kThreads = 256;     // 32 x 8
 constexpr int kTX = 64;           // tile columns (2 per thread)
 constexpr int kTY = 8;            // tile rows of apply / up / replacement tiles
-constexpr int kDTY = 16;          // fine rows of a "down" tile (8 coarse rows)
 constexpr int kHalo = 2;
 constexpr int kPW = kTX + 16;     // plane tile width: tile + 8 columns each side (16-byte aligned loads)
 constexpr int kVW = kTX + 2 * kHalo;
@@ -181,28 +180,6 @@ __device__ __forceinline__ void load_planes(T* sm, const T* g, size_t ps, int P,
     }
 }
 
-// Vector tile: ROWS x kVW values with origin (x0 - 2, y0 - 2); f(offset, gx,
-// gy) computes the value of an in-level element (loads issued together by the
-// unrolled loop), zero outside the level.
-template <int ROWS, class F>
-__device__ __forceinline__ void fill_tile(float* vt, int P, int W, int H, int x0, int y0, F f)
-{
-    constexpr int TOTAL = ROWS * kVW;
-    constexpr int ITER = (TOTAL + kThreads - 1) / kThreads;
-    float v[ITER];
-#pragma unroll
-    for (int j = 0; j < ITER; ++j) {
-        const int i = threadIdx.x + j * kThreads;
-        const int gx = x0 - kHalo + i % kVW, gy = y0 - kHalo + i / kVW;
-        v[j] = (i < TOTAL && gx >= 0 && gx < W && gy >= 0 && gy < H) ? f((size_t)gy * P + gx, gx, gy) : 0.f;
-    }
-#pragma unroll
-    for (int j = 0; j < ITER; ++j) {
-        const int i = threadIdx.x + j * kThreads;
-        if (i < TOTAL) vt[i] = v[j];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Deterministic grid reductions: each CTA publishes its partial sums, the
 // last CTA to arrive adds all partials in index order.
@@ -241,34 +218,10 @@ __device__ __forceinline__ void set_cond(const Args& a, unsigned v)
     if (a.cond) cudaGraphSetConditional((cudaGraphConditionalHandle)a.cond, v);
 }
 
-// ---------------------------------------------------------------------------
-// Stencil sums on shared-memory tiles.
-// vt: vector tile with origin (x0 - 2, y0 - 2), width kVW; pt: plane tile
-// with origin (x0 - 8, y0 - 2), width kPW, `prow` rows per plane.
-// Returns S_i = sum_j w_ij v_j at tile-local output (lx, ly), so that
-// (A v)_i = D_i v_i - S_i.  With x1 = omega b / D the smoother steps become
-//   rho = b - A x1 = (1 - omega) b + S(x1)          (D > 0; rho = b + S if D = 0)
+// The smoother steps written with 1 / D only.  With S = sum_j w_ij v_j, so
+// that (A v)_i = D_i v_i - S_i, and x1 = omega b / D:
+//   rho = b - A x1 = (1 - omega) b + S(x1)            (D > 0; rho = b + S if D = 0)
 //   x = y + omega (b - A y) / D = (1 - omega) y + omega (b + S(y)) / D
-// which need only 1 / D.
-// ---------------------------------------------------------------------------
-template <class S, class T>
-__device__ __forceinline__ float sten_sum(const T* pt, int prow, const float* vt, int lx, int ly)
-{
-    const int vc = (ly + kHalo) * kVW + lx + kHalo;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll
-    for (int k = 0; k < S::NP; ++k) {
-        const int du = S::du(k), dv = S::dv(k);
-        const float wu = tof(pt[((size_t)k * prow + ly + kHalo) * kPW + lx + 8]);
-        const float wl = tof(pt[((size_t)k * prow + ly + kHalo - dv) * kPW + lx + 8 - du]);
-        const float xu = vt[vc + dv * kVW + du];
-        const float xl = vt[vc - dv * kVW - du];
-        if (k & 1) { a1 = fmaf(wu, xu, a1); a3 = fmaf(wl, xl, a3); }
-        else { a2 = fmaf(wu, xu, a2); a0 = fmaf(wl, xl, a0); }
-    }
-    return (a0 + a2) + (a1 + a3);
-}
-
 __device__ __forceinline__ float rho_of(float b, float di, float om, float S)
 {
     return (di > 0.f ? (1.f - om) * b : b) + S;
@@ -415,47 +368,6 @@ __global__ void __launch_bounds__(kThreads, 3) mg_replace_kernel(Args a)
 // V-cycle kernels
 // ---------------------------------------------------------------------------
 
-// Level l -> l+1: x1 = omega b / D on the tile + halo, rho = b - A x1 on the
-// fine cells of each coarse cell, b_{l+1} = sum of rho over the 2x2 block.
-template <class S, class T>
-__global__ void __launch_bounds__(kThreads, 3) mg_down_kernel(Args a, int l)
-{
-    pdl_enter();
-    if (a.st->done) return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* pt = reinterpret_cast<T*>(smem);
-    float* vt = reinterpret_cast<float*>(smem + sizeof(T) * S::NP * (kDTY + kHalo) * kPW);
-    const Lev& F = a.lev[l];
-    const Lev& C = a.lev[l + 1];
-    const int W = F.W, H = F.H, P = F.P;
-    const float om = a.omega;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int tiles_x = (W + kTX - 1) / kTX, tiles = tiles_x * ((H + kDTY - 1) / kDTY);
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int x0 = (t % tiles_x) * kTX, y0 = (t / tiles_x) * kDTY;
-        __syncthreads();
-        load_planes<T, S::NP, kDTY + kHalo>(pt, static_cast<const T*>(F.c), F.ps, P, W, H, x0, y0);
-        fill_tile<kDTY + 2 * kHalo>(vt, P, W, H, x0, y0, [&](size_t o, int, int) { return om * F.b[o] * F.Di[o]; });
-        __syncthreads();
-        const int cx = (x0 >> 1) + tx, cy = (y0 >> 1) + ty;
-        if (cx < C.W && cy < C.H) {
-            float sum = 0.f;
-#pragma unroll
-            for (int bq = 0; bq < 2; ++bq)
-#pragma unroll
-                for (int aq = 0; aq < 2; ++aq) {
-                    const int lx = 2 * tx + aq, ly = 2 * ty + bq;
-                    const int gx = x0 + lx, gy = y0 + ly;
-                    if (gx < W && gy < H) {
-                        const size_t o = (size_t)gy * P + gx;
-                        sum += rho_of(F.b[o], F.Di[o], om, sten_sum<S, T>(pt, kDTY + kHalo, vt, lx, ly));
-                    }
-                }
-            C.b[(size_t)cy * C.P + cx] = sum;
-        }
-    }
-}
-
 // The small levels lt .. L of a V-cycle in ONE CTA: their operators and
 // vectors are staged in shared memory (compact [H_l][W_l] arrays) and the
 // phases (smoothing + restriction down to the coarsest level, the exact
@@ -598,42 +510,6 @@ static int tail_bytes(const int* Wl, const int* Hl, int lt, int L)
     f = (f + 1) / 2 * 2;                        // the FP64 inverse starts 8-byte aligned
     f += 2LL * Wl[L] * Hl[L] * Wl[L] * Hl[L];
     return (int)(f * 4);
-}
-
-// Level l >= 1 from x_{l+1}: y = omega b / D + scale * x_{l+1}[aggregate]
-// on the tile + halo, x = y + omega (b - A y) / D.
-template <class S, class T>
-__global__ void __launch_bounds__(kThreads, 3) mg_up_kernel(Args a, int l)
-{
-    pdl_enter();
-    if (a.st->done) return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* pt = reinterpret_cast<T*>(smem);
-    float* vt = reinterpret_cast<float*>(smem + sizeof(T) * S::NP * (kTY + kHalo) * kPW);
-    const Lev& F = a.lev[l];
-    const Lev& C = a.lev[l + 1];
-    const int W = F.W, H = F.H, P = F.P;
-    const float om = a.omega, sc = a.scale;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int tiles_x = (W + kTX - 1) / kTX, tiles = tiles_x * ((H + kTY - 1) / kTY);
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int x0 = (t % tiles_x) * kTX, y0 = (t / tiles_x) * kTY;
-        __syncthreads();
-        load_planes<T, S::NP, kTY + kHalo>(pt, static_cast<const T*>(F.c), F.ps, P, W, H, x0, y0);
-        fill_tile<kTY + 2 * kHalo>(vt, P, W, H, x0, y0, [&](size_t o, int gx, int gy) {
-            return fmaf(sc, C.x[(size_t)(gy >> 1) * C.P + (gx >> 1)], om * F.b[o] * F.Di[o]);
-        });
-        __syncthreads();
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int lx = tx + 32 * h, gx = x0 + lx, gy = y0 + ty;
-            if (gx < W && gy < H) {
-                const size_t o = (size_t)gy * P + gx;
-                const float y = vt[(ty + kHalo) * kVW + lx + kHalo];
-                F.x[o] = smooth_of(y, F.b[o], F.Di[o], om, sten_sum<S, T>(pt, kTY + kHalo, vt, lx, ty));
-            }
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1268,11 +1144,6 @@ static int occupancy(const void* fn, int smem, int threads)
     if (o < 1) o = 1;
     cache.push_back({fn, dev, smem, o});
     return o;
-}
-
-template <class T, class S> constexpr int tile_smem(int rows, int vrows)
-{
-    return (int)(sizeof(T) * S::NP * rows * kPW + sizeof(float) * vrows * kVW);
 }
 
 static int tiles_of(int W, int H, int ty) { return ((W + kTX - 1) / kTX) * ((H + ty - 1) / ty); }

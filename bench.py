@@ -433,6 +433,20 @@ def run_ours(args):
                       "solve_ms": sum(r.kernel_ms for r in res_m) / args.steps,
                       "speedup_vs_cg": (1000 * t_max / args.steps) / (sum(ms_m) / args.steps),
                       "solve_only_ms": timed_solve("mg", args.steps)[0]}
+        # end to end through the public API from pinned host buffers, like `e2e`
+        def step_mg_e2e():
+            img_d.copy_(img_h, non_blocking=True)
+            scr_d.copy_(scr_h, non_blocking=True)
+            alpha.copy_(a0_h, non_blocking=True)
+            store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
+            r = store.solve(alpha, "mg", **params)
+            out_h.copy_(alpha, non_blocking=True)
+            return r
+
+        step_mg_e2e()
+        ms_me, res_me = timed(step_mg_e2e, args.steps)
+        assert all(r.status == 0 and (args.fixed_iters or r.rel_residual <= 1e-6) for r in res_me), res_me
+        line["mg"]["e2e_ms"] = sum(ms_me) / args.steps
         # the same multigrid solve with the V-cycle on the FP32 planes (use_low = 0)
         ms32, res32 = timed_solve("mg", args.steps, use_low=0)
         line["mg"]["fp32_planes"] = {"solve_only_ms": ms32, "iters": res32[0].iters,

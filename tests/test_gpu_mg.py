@@ -244,6 +244,23 @@ def test_mg_many_matches_single_solves(orc):
             assert np.array_equal(a.cpu().numpy().view(np.uint32), ref.view(np.uint32))
 
 
+def test_mg_many_rejects_mixed_precisions_and_empty(orc):
+    torch = torch_cuda()
+    from gpumatting_b200 import _lib as L
+    from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
+
+    q = make_problem(64, 48, 3)
+    img, scr = torch.from_numpy(q.image).cuda(), torch.from_numpy(q.scribbles).cuda()
+    a16 = api.LevinStore(64, 48, "fp16").assemble(img, scr, eps=q.eps)
+    a32 = api.LevinStore(64, 48, "fp32").assemble(img, scr, eps=q.eps)
+    alphas = [torch.full((48, 64), 0.5, device="cuda") for _ in range(2)]
+    with pytest.raises(L.GmError) as e:
+        api.mg_solve_many([a16, a32], alphas)
+    assert e.value.status == L.GM_ERR_INVALID
+    assert api.mg_solve_many([], []) == []
+
+
 def test_mg_rejected_where_unsupported(orc):
     torch = torch_cuda()
     from gpumatting_b200 import _lib as L

@@ -61,3 +61,35 @@ def test_mgpcg_converges_and_beats_cg(orc):
     assert np.linalg.norm(b - op.apply(x.ravel())) / np.linalg.norm(b) <= 1.001e-6
     _, it_cg, _ = op.cg(b, np.full(W * H, 0.5), rtol=1e-6, maxit=20000)
     assert it * 4 < it_cg, (it, it_cg)
+
+
+@pytest.mark.parametrize("W,H", [(1920, 1080), (4096, 4096), (37, 29), (8, 2), (1, 1), (1000, 3), (130, 3)])
+def test_level_shapes_match_oracle(W, H):
+    """gm_levin_mg_levels (host only, no device call) lists the oracle's
+    hierarchy: 2x2 coarsening until a level has at most 128 cells."""
+    import ctypes as C
+
+    from gpumatting_b200 import _lib as L
+    from oracle import mg as M
+
+    n = C.c_int(0)
+    dims = (C.c_int * 64)()
+    assert L.load().gm_levin_mg_levels(W, H, C.byref(n), dims, 32) == 0
+    got = [(dims[2 * i], dims[2 * i + 1]) for i in range(n.value)]
+    want = [(W, H)]
+    while True:
+        w, h = want[-1]
+        want.append(((w + 1) // 2, (h + 1) // 2))
+        if want[-1][0] * want[-1][1] <= M.COARSE_MAX:
+            break
+    assert got == want
+
+
+def test_level_shapes_reject_bad_sizes():
+    import ctypes as C
+
+    from gpumatting_b200 import _lib as L
+
+    n = C.c_int(0)
+    assert L.load().gm_levin_mg_levels(0, 5, C.byref(n), None, 0) == L.GM_ERR_INVALID
+    assert L.load().gm_levin_mg_levels(5, -1, C.byref(n), None, 0) == L.GM_ERR_INVALID

@@ -254,7 +254,7 @@ typedef struct gm_solve_params_s {
     int use_low;          /* mixed store: 1 = iterate with the low-precision planes */
     double timeout_s;     /* limit on any single wait inside the kernel     */
     int ctas_per_sm;      /* 0 = auto                                      */
-    int strip_width;      /* columns per CTA strip, multiple of 8, <= 240 (0 = auto) */
+    int strip_width;      /* reserved, ignored: the fused solver's strips are 192 columns */
     int inject;           /* test hook, 0 in normal use: 1 = the first grid barrier
                              waits for one arrival that never comes, so the call
                              must end with GM_ERR_TIMEOUT after timeout_s */

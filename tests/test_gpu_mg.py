@@ -261,6 +261,26 @@ def test_mg_many_rejects_mixed_precisions_and_empty(orc):
     assert api.mg_solve_many([], []) == []
 
 
+def test_mg_breakdown_status(orc):
+    """A non-finite value in the operator ends the solve with GM_ERR_BREAKDOWN
+    (no hang, the context stays usable)."""
+    torch = torch_cuda()
+    from gpumatting_b200 import _lib as L
+
+    W, H = 64, 48
+    st, p, w, g, b = _store(orc, W, H, "fp16")
+    st.planes("gamma")[10, 10] = float("nan")
+    torch.cuda.synchronize()
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    with pytest.raises(L.GmError) as e:
+        st.solve(alpha, "mg", rtol=1e-6)
+    assert e.value.status == L.GM_ERR_BREAKDOWN
+    st2, p2, w2, g2, b2 = _store(orc, W, H, "fp16", seed=3)
+    alpha.fill_(0.5)
+    r = st2.solve(alpha, "mg", rtol=1e-6)
+    assert r.status == 0 and r.rel_residual <= 1e-6
+
+
 def test_mg_rejected_where_unsupported(orc):
     torch = torch_cuda()
     from gpumatting_b200 import _lib as L

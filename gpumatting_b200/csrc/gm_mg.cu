@@ -78,7 +78,8 @@ struct CoarseSten {
 // Device-resident solver state (scalars of the outer PCG).
 struct State {
     double rz, pq, alpha, beta, rr, bn2, rr_true;
-    int iter, done, status, need_replace, replacements, pad_;
+    int iter, done, status, need_replace, replacements;
+    int fold_at;  // iteration whose update folds the FP32 increment into x
     unsigned ticket[8];
 };
 enum { T_PQ = 0, T_RR = 1, T_TRUE = 2, T_RZ = 3 };
@@ -109,7 +110,8 @@ struct Args {
     int bpitch;
     const float* alpha_in;
     float* alpha_out;     // [H][W]
-    double* x;            // FP64 solution [H][P]
+    double* x;            // FP64 solution [H][P]; the solution is x + xinc
+    float* xinc;          // FP32 increment since the last replacement [H][P]
     float *r, *q, *p0, *p1;  // fine vectors [H][P]; z is lev[0].x
     double* minv;         // coarsest inverse [n][n]
     double* parts;        // [5][kMaxParts]: pq, rr, true rr + bb, rz
@@ -249,6 +251,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(Args a)
     const double al = st->alpha;
     const float alf = (float)al;
     const float* pn = (it & 1) ? a.p0 : a.p1;
+    const bool fold = st->fold_at == it;  // a replacement ran: move the increment into x
     double acc = 0.0;
     const int qpr = (W + 3) / 4;
     const size_t nq = (size_t)qpr * H;
@@ -258,19 +261,28 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(Args a)
         const float4 p = *reinterpret_cast<const float4*>(pn + o);
         const float4 q = *reinterpret_cast<const float4*>(a.q + o);
         float4 r = *reinterpret_cast<const float4*>(a.r + o);
-        double2 x01 = *reinterpret_cast<const double2*>(a.x + o);
-        double2 x23 = *reinterpret_cast<const double2*>(a.x + o + 2);
+        float4 xi = *reinterpret_cast<const float4*>(a.xinc + o);
         const bool v1 = x + 1 < W, v2 = x + 2 < W, v3 = x + 3 < W;
-        x01.x += al * (double)p.x;
-        x01.y = v1 ? x01.y + al * (double)p.y : 0.0;
-        x23.x = v2 ? x23.x + al * (double)p.z : 0.0;
-        x23.y = v3 ? x23.y + al * (double)p.w : 0.0;
+        if (fold) {
+            double2 x01 = *reinterpret_cast<const double2*>(a.x + o);
+            double2 x23 = *reinterpret_cast<const double2*>(a.x + o + 2);
+            x01.x += (double)xi.x;
+            x01.y = v1 ? x01.y + (double)xi.y : 0.0;
+            x23.x = v2 ? x23.x + (double)xi.z : 0.0;
+            x23.y = v3 ? x23.y + (double)xi.w : 0.0;
+            *reinterpret_cast<double2*>(a.x + o) = x01;
+            *reinterpret_cast<double2*>(a.x + o + 2) = x23;
+            xi = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        xi.x = fmaf(alf, p.x, xi.x);
+        xi.y = v1 ? fmaf(alf, p.y, xi.y) : 0.f;
+        xi.z = v2 ? fmaf(alf, p.z, xi.z) : 0.f;
+        xi.w = v3 ? fmaf(alf, p.w, xi.w) : 0.f;
         r.x = fmaf(-alf, q.x, r.x);
         r.y = v1 ? fmaf(-alf, q.y, r.y) : 0.f;
         r.z = v2 ? fmaf(-alf, q.z, r.z) : 0.f;
         r.w = v3 ? fmaf(-alf, q.w, r.w) : 0.f;
-        *reinterpret_cast<double2*>(a.x + o) = x01;
-        *reinterpret_cast<double2*>(a.x + o + 2) = x23;
+        *reinterpret_cast<float4*>(a.xinc + o) = xi;
         *reinterpret_cast<float4*>(a.r + o) = r;
         acc += (double)r.x * r.x + (double)r.y * r.y + ((double)r.z * r.z + (double)r.w * r.w);
     }
@@ -309,7 +321,8 @@ __global__ void __launch_bounds__(kThreads, 3) mg_replace_kernel(Args a)
         for (int j = 0; j < XI; ++j) {
             const int i = threadIdx.x + j * kThreads;
             const int gx = x0 - kHalo + i % kVW, gy = y0 - kHalo + i / kVW;
-            xv[j] = (i < XT && gx >= 0 && gx < W && gy >= 0 && gy < H) ? a.x[(size_t)gy * P + gx] : 0.0;
+            const size_t o = (size_t)gy * P + gx;
+            xv[j] = (i < XT && gx >= 0 && gx < W && gy >= 0 && gy < H) ? a.x[o] + (double)a.xinc[o] : 0.0;
         }
 #pragma unroll
         for (int j = 0; j < XI; ++j) {
@@ -344,6 +357,7 @@ __global__ void __launch_bounds__(kThreads, 3) mg_replace_kernel(Args a)
     if (last_cta_total<2>(v, a.parts + 2 * kMaxParts, &st->ticket[T_TRUE]) && threadIdx.x == 0) {
         if (st->replacements == 0) st->bn2 = v[1];
         st->replacements += 1;
+        st->fold_at = st->iter;
         st->need_replace = 0;
         st->rr_true = v[0];
         st->rr = v[0];
@@ -666,11 +680,11 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
             } else {
                 v = om * v0b[i] * v1b[i];  // x1 = omega b / d (v1 holds 1 / d)
                 if (MODE == FM_UP) {
+                    // 1/d is zero outside the image (zero fill) and on pixels
+                    // with no coupling and no scribble: y = 0 there
                     const int row = i / kFBW, col = i - row * kFBW;
-                    const int gu = u0 - 8 + col, gv = v0 - 2 + row;
                     const float* xb = reinterpret_cast<const float*>(sp + LY::x_off);
-                    v = (gu >= 0 && gu < W && gv >= 0 && gv < H) ? fmaf(sc, xb[(row >> 1) * kXBW + (col >> 1)], v)
-                                                                   : 0.f;
+                    v = v1b[i] > 0.f ? fmaf(sc, xb[(row >> 1) * kXBW + (col >> 1)], v) : 0.f;
                 }
             }
             vt[i] = v;
@@ -944,6 +958,7 @@ __global__ void mg_init_kernel(Args a)
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int y = (int)(i / W), x = (int)(i % W);
         a.x[(size_t)y * P + x] = (double)a.alpha_in[(size_t)y * W + x];
+        a.xinc[(size_t)y * P + x] = 0.f;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         State* st = a.st;
@@ -953,6 +968,7 @@ __global__ void mg_init_kernel(Args a)
         st->status = GM_OK;
         st->need_replace = 1;
         st->replacements = 0;
+        st->fold_at = -1;
         for (int k = 0; k < 8; ++k) st->ticket[k] = 0u;
     }
 }
@@ -966,7 +982,8 @@ __global__ void mg_final_kernel(Args a)
     const size_t n = (size_t)W * H;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int y = (int)(i / W), x = (int)(i % W);
-        a.alpha_out[(size_t)y * W + x] = zero ? 0.f : (float)a.x[(size_t)y * P + x];
+        const size_t o = (size_t)y * P + x;
+        a.alpha_out[(size_t)y * W + x] = zero ? 0.f : (float)(a.x[o] + (double)a.xinc[o]);
     }
 }
 
@@ -1019,9 +1036,10 @@ static size_t carve(const Plan& pl, int P0, char* base, Args* a)
     float* p1 = (float*)take(n0 * 4);
     float* z = (float*)take(n0 * 4);
     float* di0 = (float*)take(n0 * 4);
+    float* xinc = (float*)take(n0 * 4);
     double* x = (double*)take(n0 * 8);
     if (a) {
-        a->r = r; a->q = q; a->p0 = p0; a->p1 = p1; a->x = x;
+        a->r = r; a->q = q; a->p0 = p0; a->p1 = p1; a->x = x; a->xinc = xinc;
         a->lev[0].b = r;
         a->lev[0].x = z;
         a->lev[0].Di = di0;

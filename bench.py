@@ -495,11 +495,11 @@ def run_ours(args):
 
 
 # Multigrid PCG, algorithmic bytes per pixel-iteration: SpMV 68 (FP32 planes
-# 48, d32, z and p read, p and q written), update 32 (x FP64 read/write, p,
-# q, r read, r written), level-0 restriction 33 and prolongation 37 (FP16
-# planes 24, r, 1/d, the coarse side, z written), coarse levels 18 (54 B per
-# coarse cell, a third of a pixel).
-MG_BYTES_PER_PX_ITER = 68 + 32 + 33 + 37 + 18
+# 48, d32, z and p read, p and q written), update 24 (FP32 solution increment
+# read/write, p, q, r read, r written), level-0 restriction 33 and
+# prolongation 37 (FP16 planes 24, r, 1/d, the coarse side, z written),
+# coarse levels 18 (54 B per coarse cell, a third of a pixel).
+MG_BYTES_PER_PX_ITER = 68 + 24 + 33 + 37 + 18
 
 # Algorithmic bytes per pixel of one SpMV pass: band planes + diagonal plane
 # + x read once + y written once.

@@ -588,6 +588,18 @@ template <> __device__ __forceinline__ float2 ld2<__nv_bfloat16>(const __nv_bflo
     return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
 }
 
+// Adds expected TMA bytes to the current phase without arriving; and a plain
+// arrival (the phase completes once its bytes have landed).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_only(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Waits for a TMA stage with a wall-clock limit (2 s); on expiry the solve
 // ends with GM_ERR_TIMEOUT.
 __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, State* st)
@@ -615,12 +627,6 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
     constexpr int TH = LY::TH, NT = LY::THR, RPT = TH / (NT / 64);
     static_assert(RPT == 2, "each thread covers one row pair");
     constexpr int PW = (TH + 2) * kFBW;  // elements per plane in the box
-    pdl_enter();
-    State* st = a.st;
-    if (st->done) {
-        if (MODE == FM_UP && blockIdx.x == 0 && threadIdx.x == 0) set_cond(a, 0u);
-        return;
-    }
     // TMA destinations must be 128-byte aligned; the dynamic region follows
     // the reduction's static shared memory, so align its base by hand.
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -630,33 +636,61 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
     const Lev& F = a.lev[l];
     const int W = F.W, H = F.H, P = F.P, tid = threadIdx.x, G = gridDim.x;
     const int ntx = (W + kFTW - 1) / kFTW, ntiles = ntx * ((H + TH - 1) / TH);
-    const int it = st->iter;
-    const bool first = it == 0;
-    const float beta = (float)st->beta, om = a.omega, sc = a.scale;
-    const CUtensorMap* mv1 = MODE == FM_SPMV ? ((it & 1) ? &tm.m[3] : &tm.m[2]) : &tm.m[2];
-    float* pnew = (it & 1) ? a.p0 : a.p1;
-    const Lev& C = a.lev[l + 1];
+    const int t0 = blockIdx.x;
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
         fence_mbar_init();
     }
     __syncthreads();
-    auto issue = [&](int t, int s) {
+    auto issue_planes = [&](int t, int s) {
+        const int u0 = (t % ntx) * kFTW, v0 = (t / ntx) * TH;
+        tma_load_3d(smem + s * LY::stage, &tm.m[0], u0 - 8, v0 - 2, 0, &full[s]);
+    };
+    // The planes are constant during a solve (written by the store's assembly
+    // or the set-up kernels, which completed before this kernel's predecessor
+    // began), so the first two stages' plane boxes are requested before the
+    // wait for the predecessor; the stage's arrival comes with the vectors.
+    const int npre = (t0 < ntiles ? 1 : 0) + (t0 + G < ntiles ? 1 : 0);
+    if (tid == 0)
+        for (int k = 0; k < npre; ++k) {
+            mbar_expect_tx(&full[k], (uint32_t)LY::PB);
+            issue_planes(t0 + k * G, k);
+        }
+    pdl_enter();
+    State* st = a.st;
+    if (st->done) {
+        if (MODE == FM_UP && blockIdx.x == 0 && threadIdx.x == 0) set_cond(a, 0u);
+        // complete the stages with no vectors and let the plane loads land
+        if (tid == 0)
+            for (int k = 0; k < npre; ++k) mbar_arrive_only(&full[k]);
+        for (int k = 0; k < npre; ++k) stage_wait(&full[k], 0u, st);
+        return;
+    }
+    const int it = st->iter;
+    const bool first = it == 0;
+    const float beta = (float)st->beta, om = a.omega, sc = a.scale;
+    const CUtensorMap* mv1 = MODE == FM_SPMV ? ((it & 1) ? &tm.m[3] : &tm.m[2]) : &tm.m[2];
+    float* pnew = (it & 1) ? a.p0 : a.p1;
+    const Lev& C = a.lev[l + 1];
+    auto issue_vectors = [&](int t, int s) {
         const int u0 = (t % ntx) * kFTW, v0 = (t / ntx) * TH;
         unsigned char* sp = smem + s * LY::stage;
-        mbar_arrive_expect_tx(&full[s], LY::bytes);
-        tma_load_3d(sp, &tm.m[0], u0 - 8, v0 - 2, 0, &full[s]);
         tma_load_2d(sp + LY::v0_off, &tm.m[1], u0 - 8, v0 - 2, &full[s]);
         tma_load_2d(sp + LY::v1_off, mv1, u0 - 8, v0 - 2, &full[s]);
         if (MODE == FM_UP) tma_load_2d(sp + LY::x_off, &tm.m[3], u0 / 2 - 4, v0 / 2 - 1, &full[s]);
         if (MODE == FM_SPMV) tma_load_2d(sp + LY::d_off, &tm.m[4], u0, v0, &full[s]);
     };
-    const int t0 = blockIdx.x;
-    if (tid == 0 && t0 < ntiles) {
-        issue(t0, 0);
-        if (t0 + G < ntiles) issue(t0 + G, 1);
-    }
+    auto issue = [&](int t, int s) {
+        mbar_arrive_expect_tx(&full[s], LY::bytes);
+        issue_planes(t, s);
+        issue_vectors(t, s);
+    };
+    if (tid == 0)
+        for (int k = 0; k < npre; ++k) {
+            mbar_arrive_expect_tx(&full[k], LY::bytes - (uint32_t)LY::PB);
+            issue_vectors(t0 + k * G, k);
+        }
     const int cp = tid & 63, rg = tid >> 6;
     const int lu = 8 + 2 * cp;
     const int r0 = rg * RPT;

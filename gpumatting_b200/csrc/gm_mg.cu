@@ -18,20 +18,26 @@
 //
 // V-cycle on level l with right-hand side b: x1 = omega b / D,
 // b_{l+1} = P^T (b - A x1), recurse, y = x1 + scale P x_{l+1},
-// x = y + omega (b - A y) / D.  Each level costs two streaming kernels
-// ("down": smoothing + residual + restriction; "up": prolongation + smoothing);
-// x1 is recomputed from b in "up" instead of stored.
+// x = y + omega (b - A y) / D.  Each level above the tail costs two streaming
+// kernels ("down": smoothing + residual + restriction; "up": prolongation +
+// smoothing), both the persistent TMA-ring stencil kernel mg_fine_kernel; x1
+// is recomputed from b in "up" instead of stored.  The small levels at the
+// bottom (up to 160 KB of operators) run in one CTA (mg_tail_kernel), staged
+// in shared memory with block barriers between their phases.
 //
-// Outer loop: PCG with FP64 solution, FP32 vectors and FP64 scalars on the
-// true FP32 operator; only the preconditioner reads the low-precision planes
-// (the few MG iterations make the outer operator's bytes minor, and a BF16
-// outer operator would stall the recurrence).  The true residual b - A x in
-// FP64 arithmetic replaces the recurrence every `replace_every` iterations and
-// decides convergence (the same reliable-update rule as the fused CG).
+// Outer loop: PCG with FP64 solution (plus an FP32 increment folded in after
+// each replacement), FP32 vectors and FP64 scalars on the true FP32 operator;
+// only the preconditioner reads the low-precision planes (the few MG
+// iterations make the outer operator's bytes minor, and a BF16 outer operator
+// would stall the recurrence).  The true residual b - A x in FP64 arithmetic
+// replaces the recurrence every `replace_every` iterations and decides
+// convergence (the same reliable-update rule as the fused CG).
 // All scalars stay on the device: every reduction ends in the last CTA to
 // finish (fixed summation order, so results are deterministic), and the whole
 // solve is ONE CUDA graph launch whose iteration loop is a device-side
-// conditional WHILE node -- no host round trip per iteration.
+// conditional WHILE node -- no host round trip per iteration.  Kernels are
+// chained with programmatic dependent launch.  gm_levin_solve_mg_many runs
+// many such solves on concurrent streams.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>

@@ -281,6 +281,43 @@ def test_mg_breakdown_status(orc):
     assert r.status == 0 and r.rel_residual <= 1e-6
 
 
+_HOST_LOOP_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from gpumatting_b200 import api
+from gpumatting_b200.synth import make_problem
+q = make_problem(160, 120, 4)
+st = api.LevinStore(160, 120, "fp16").assemble(torch.from_numpy(q.image).cuda(), torch.from_numpy(q.scribbles).cuda(),
+                                               eps=q.eps)
+a = torch.full((120, 160), 0.5, device="cuda")
+r = st.solve(a, "mg", rtol=1e-6, max_iters=2000)
+np.save(sys.argv[2], a.cpu().numpy())
+print(r.iters, r.status)
+"""
+
+
+def test_mg_host_loop_matches_graph(orc, tmp_path):
+    """GM_MG_GRAPH=0 (the same kernels launched one by one, the done flag
+    read every 4 iterations) gives the graph path's result bit for bit."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for mode in ("1", "0"):
+        path = str(tmp_path / f"alpha_{mode}.npy")
+        env = dict(os.environ, GM_MG_GRAPH=mode)
+        res = subprocess.run([sys.executable, "-c", _HOST_LOOP_SCRIPT, root, path], env=env, capture_output=True,
+                             text=True, timeout=300)
+        assert res.returncode == 0, res.stderr[-2000:]
+        iters, status = res.stdout.split()[-2:]
+        assert status == "0"
+        outs[mode] = (int(iters), np.load(path))
+    assert outs["0"][0] == outs["1"][0]
+    assert np.array_equal(outs["0"][1].view(np.uint32), outs["1"][1].view(np.uint32))
+
+
 def test_mg_rejected_where_unsupported(orc):
     torch = torch_cuda()
     from gpumatting_b200 import _lib as L

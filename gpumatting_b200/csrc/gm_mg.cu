@@ -86,6 +86,7 @@ struct State {
     double rz, pq, alpha, beta, rr, bn2, rr_true;
     int iter, done, status, need_replace, replacements;
     int fold_at;  // iteration whose update folds the FP32 increment into x
+    int restart;  // the next search direction is z alone (beta = 0)
     unsigned ticket[8];
 };
 enum { T_PQ = 0, T_RR = 1, T_TRUE = 2, T_RZ = 3 };
@@ -365,6 +366,14 @@ __global__ void __launch_bounds__(kThreads, 3) mg_replace_kernel(Args a)
         st->replacements += 1;
         st->fold_at = st->iter;
         st->need_replace = 0;
+        // A true residual well above the recurrence's (more than twice its
+        // norm) means the FP32 recurrences drifted: from a zero guess the
+        // first cycle can carry the whole solution in the FP32 increment.
+        // The old direction is then conjugate to a residual that no longer
+        // exists, and beta = true r.z / recurrence r.z would let it swamp
+        // the new one (the iteration stalls), so the next direction restarts
+        // from z.  Forward solves never open such a gap.
+        st->restart = v[0] > 4.0 * st->rr;
         st->rr_true = v[0];
         st->rr = v[0];
         const double bn2 = st->bn2;
@@ -838,7 +847,8 @@ __global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)si
         double v[1] = {acc};
         if (last_cta_total<1>(v, a.parts + 4 * kMaxParts, &st->ticket[T_RZ]) && threadIdx.x == 0) {
             const double rz = v[0];
-            if (st->iter > 0) st->beta = rz / st->rz;
+            if (st->iter > 0) st->beta = st->restart ? 0.0 : rz / st->rz;
+            st->restart = 0;
             st->rz = rz;
             if (!isfinite(rz)) {
                 st->status = GM_ERR_BREAKDOWN;
@@ -1009,6 +1019,7 @@ __global__ void mg_init_kernel(Args a)
         st->need_replace = 1;
         st->replacements = 0;
         st->fold_at = -1;
+        st->restart = 0;
         for (int k = 0; k < 8; ++k) st->ticket[k] = 0u;
     }
 }

@@ -1,8 +1,12 @@
-"""The drop-in C-ABI from C: tests/c/test_dropin.c follows the reference's
-main.cu call sequence (hostLevinLaplacian, bmCopyToDevice, vecCopyToDevice,
-cgSolve / gradSolve, computeError, the frees).  It is compiled with gcc
-against include/gpumat.h and the in-tree libgpumat.so here (the header is
-plain C) and run on the GPU."""
+"""The C-ABI from C, compiled with gcc against include/gpumat.h and the
+in-tree libgpumat.so (the header is plain C) and run on the GPU.
+
+tests/c/test_dropin.c follows the reference's main.cu call sequence
+(hostLevinLaplacian, bmCopyToDevice, vecCopyToDevice, cgSolve / gradSolve,
+computeError, the frees).  tests/c/test_native.c drives the native store API
+(gm_levin_store_alloc, gm_levin_assemble, gm_levin_solve with CG / PCG / MG,
+gm_levin_solve_mg_many, a gm_batch solve, gm_levin_adjoint) and checks each
+solution on the host with an FP64 residual of the store's FP32 planes."""
 import os
 import shutil
 import subprocess
@@ -11,28 +15,41 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+PROGRAMS = ("test_dropin", "test_native")
 
 
-def _build(out: str) -> None:
+def _build(name: str, out: str) -> None:
     if shutil.which("gcc") is None:
         pytest.skip("gcc not available")
     lib = os.path.join(ROOT, "gpumatting_b200")
     cmd = ["gcc", "-std=c99", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
-           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "c", "test_dropin.c"),
+           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "c", name + ".c"),
            "-L", lib, "-lgpumat", "-L", os.path.join(CUDA, "lib64"), "-lcudart",
            f"-Wl,-rpath,{lib}", f"-Wl,-rpath,{os.path.join(CUDA, 'lib64')}", "-lm", "-o", out]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
 
 
-def test_c_program_compiles_and_links(tmp_path):
-    _build(str(tmp_path / "test_dropin"))
+@pytest.mark.parametrize("name", PROGRAMS)
+def test_c_program_compiles_and_links(tmp_path, name):
+    _build(name, str(tmp_path / name))
+
+
+def _run(tmp_path, name: str) -> str:
+    exe = str(tmp_path / name)
+    _build(name, exe)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0 and "Test PASSED" in r.stdout, r.stdout + r.stderr
+    return r.stdout
 
 
 @pytest.mark.gpu
 def test_c_program_runs_the_reference_sequence(tmp_path):
-    exe = str(tmp_path / "test_dropin")
-    _build(exe)
-    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
-    print(r.stdout)
-    assert r.returncode == 0 and "Test PASSED" in r.stdout, r.stdout + r.stderr
-    assert "Ground truth MSE" in r.stdout
+    assert "Ground truth MSE" in _run(tmp_path, "test_dropin")
+
+
+@pytest.mark.gpu
+def test_c_program_drives_the_native_store_api(tmp_path):
+    out = _run(tmp_path, "test_native")
+    for what in ("CG:", "PCG:", "MG:", "mg_many[1]:", "batch[1]:", "adjoint:"):
+        assert what in out

@@ -163,6 +163,53 @@ def test_mg_adjoint_matches_cg_adjoint(orc):
         assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_)
 
 
+def _edge_image(W, H, seed=0):
+    """RGB8 soft edge with +-4 noise and column strokes (the problem of
+    tests/c/test_native.c)."""
+    v, u = np.mgrid[0:H, 0:W]
+    a = 1.0 / (1.0 + np.exp(-(u - W // 2 + 5.0 * np.sin(v * 0.17 + seed)) / 2.0))
+    i = (u + v * W).astype(np.int64)
+    fg, bg = np.array([230.0, 60.0, 30.0]), np.array([25.0, 80.0, 200.0])
+    img = np.empty((H, W, 3), np.uint8)
+    for c in range(3):
+        n = ((i * 7919 + c * 104729 + seed * 31) % 2**32) % 9 - 4
+        val = a * fg[c] + (1 - a) * bg[c] + n
+        img[..., c] = np.clip(np.floor(val + 0.5), 0, 255).astype(np.uint8)
+    sc = np.full((H, W), 128, np.uint8)
+    sc[(u >= W - 6) & (u < W - 2) & (v % 3 != 0)] = 255
+    sc[(u >= 2) & (u < 6) & (v % 3 != 1)] = 0
+    return img, sc
+
+
+def test_mg_constant_rhs_from_zero_guess(orc):
+    """The adjoint of loss = sum(alpha) solves A lambda = 1/2 from lambda = 0.
+    lambda reaches ~190 there, so the first 50 iterations carry it all in the
+    FP32 increment and the first true residual is ~100x the recurrence's; the
+    solver must restart its direction there instead of stalling near 1e-4
+    (which it did, hitting max_iters)."""
+    torch = torch_cuda()
+    from gpumatting_b200 import api
+
+    W, H = 96, 64
+    img, sc = _edge_image(W, H)
+    st = api.LevinStore(W, H, "fp16").assemble(torch.from_numpy(img).cuda(), torch.from_numpy(sc).cuda(), eps=1e-5,
+                                               gamma_value=100.0)
+    rhs = torch.full((H, W), 0.5, device="cuda")
+    lam = torch.zeros((H, W), device="cuda")
+    res = st.solve_rhs(rhs, lam, "mg", rtol=1e-6, max_iters=300)
+    assert res.status == 0 and res.rel_residual <= 1e-6 and res.iters <= 100, res
+    # FP64 residual of the returned FP32 lambda: its rounding alone leaves ~3e-5
+    g = np.where(sc != 128, 100.0, 0.0).ravel()
+    rel, _ = _true_relres(orc, st, g, np.full(W * H, 0.5), lam.double().cpu().numpy().ravel())
+    assert rel <= 1e-4, rel
+    assert float(lam.max()) > 100.0  # the large solution this case is about
+    # and the adjoint through the same solve reports convergence
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    assert st.solve(alpha, "mg", rtol=1e-6).status == 0
+    _, _, _, ra = st.adjoint(alpha, torch.full((H, W), 0.5, device="cuda"), "mg", rtol=1e-6, max_iters=300)
+    assert ra.status == 0, ra
+
+
 def test_mg_on_restricted_store_matches_fp64_elimination(orc):
     """Hard constraints (gm_levin_restrict) then MG-PCG to 1e-10: within 1e-4
     of the FP64 elimination of the known pixels."""

@@ -166,8 +166,9 @@ enum { GM_PREC_FP32 = 0, GM_PREC_FP16 = 1, GM_PREC_BF16 = 2 };
  * GM_SOLVER_MG: CG preconditioned with an aggregation multigrid V-cycle
  * (2x2 piecewise-constant aggregates, Galerkin coarse operators, one damped
  * Jacobi step before and after each coarse correction, exact solve of the
- * coarsest level of <= 128 cells); single symmetric-store solves only
- * (gm_levin_solve, gm_levin_solve_rhs, gm_levin_adjoint).  The reference
+ * coarsest level of <= 128 cells); symmetric stores (gm_levin_solve,
+ * gm_levin_solve_rhs, gm_levin_adjoint, gm_levin_solve_mg_many) and batches
+ * (gm_batch_solve, one graph launch per image).  The reference
  * sketches aggregation operators over superpixels for this purpose
  * (gridoperators.h:18-138, SLIC.cpp:32, commented out at main.cu:201-218)
  * without finishing them. */
@@ -393,7 +394,10 @@ int gm_batch_tune(gm_batch* b, const gm_solve_params* p, int iters, void* stream
  * change).  alphas: host array of `count` device pointers ([H_k][W_k],
  * initial guess in, solution out); infos: `count` results (kernel_ms and
  * grid are those of the one launch).  p->ctas_per_sm = 0 uses the tuned
- * shape (tuning on first use).  Returns the worst per-image status. */
+ * shape (tuning on first use).  Returns the worst per-image status.
+ * GM_SOLVER_MG runs gm_levin_solve_mg_many over the images' store views
+ * instead (one graph launch per image on concurrent streams; kernel_ms is
+ * the whole set's time). */
 int gm_batch_solve(gm_batch* b, float* const* alphas, const gm_solve_params* p, gm_solve_info* infos,
                    void* stream);
 /* Tuned shape (0 / -1 before tuning), graph launches so far, last grid. */

@@ -365,11 +365,31 @@ def test_mg_host_loop_matches_graph(orc, tmp_path):
     assert np.array_equal(outs["0"][1].view(np.uint32), outs["1"][1].view(np.uint32))
 
 
-def test_mg_rejected_where_unsupported(orc):
+def test_batch_solve_with_mg(orc):
+    """gm_batch_solve with GM_SOLVER_MG gives every image of the canvas its own
+    one-graph MG solve (concurrent streams): each result matches, bit for bit
+    and in iterations, a solve of that image's store view alone."""
+    import ctypes as C
+
     torch = torch_cuda()
     from gpumatting_b200 import _lib as L
     from gpumatting_b200 import api
+    from gpumatting_b200.synth import make_problem
 
-    batch = api.LevinBatch([(64, 48)], "fp16")
-    with pytest.raises(L.GmError):
-        batch.solve([torch.full((48, 64), 0.5, device="cuda")], "mg")
+    sizes = [(70, 41), (96, 64), (33, 90)]
+    b = api.LevinBatch(sizes, "fp16")
+    for k, (w, h) in enumerate(sizes):
+        q = make_problem(w, h, 40 + k)
+        b.assemble(k, torch.from_numpy(q.image).cuda(), torch.from_numpy(q.scribbles).cuda(), eps=q.eps)
+    outs = [torch.full((h, w), 0.5, device="cuda") for w, h in sizes]
+    res = b.solve(outs, "mg", rtol=1e-6, max_iters=2000)
+    prm = L.default_params(solver=L.GM_SOLVER_MG, rtol=1e-6, max_iters=2000)
+    for k, (w, h) in enumerate(sizes):
+        assert res[k].status == 0 and res[k].rel_residual <= 1e-6, res[k]
+        view = b.store_view(k)
+        a = torch.full((h, w), 0.5, device="cuda")
+        info = L.GmSolveInfo()
+        rc = L.load().gm_levin_solve(C.byref(view), a.data_ptr(), C.byref(prm), C.byref(info),
+                                     torch.cuda.current_stream().cuda_stream)
+        assert rc == 0 and info.iters == res[k].iters, (info.as_dict(), res[k])
+        assert np.array_equal(a.cpu().numpy().view(np.uint32), outs[k].cpu().numpy().view(np.uint32))

@@ -176,3 +176,58 @@ def mgpcg(levels, op_apply, b: np.ndarray, x0: np.ndarray, rtol: float = 1e-6, m
         p = z + (rz1 / rz) * p
         rz = rz1
     return x, maxit, np.linalg.norm(r) / bn
+
+
+def mgpcg_fp32(levels, op_true, apply32, b: np.ndarray, x0: np.ndarray, rtol: float = 1e-6, maxit: int = 500,
+               replace_every: int = 50, restart_gap: bool = True, omega: float = OMEGA, scale: float = SCALE):
+    """The GPU solver's arithmetic scheme around the same V-cycle, for
+    checking its update rules on the CPU (the V-cycle itself stays FP64 here).
+
+    FP64 solution x plus an FP32 increment; FP32 r, p, q; FP64 scalars;
+    apply32(p) the FP32 outer operator.  Every `replace_every` iterations and
+    at apparent convergence the increment folds into x and the FP64 true
+    residual b - op_true(x) replaces r; convergence is declared only there.
+    restart_gap: a replacement whose true residual norm exceeds twice the
+    recurrence's sets beta = 0 for the next direction (the GPU rule);
+    without it beta = (true r.z) / (recurrence r.z).  Returns (x, iterations,
+    true relative residual)."""
+    f32 = np.float32
+    H, W = levels[0].H, levels[0].W
+    bb = np.asarray(b, np.float64).ravel()
+    bn2 = float(bb @ bb)
+    x = np.asarray(x0, np.float64).ravel().copy()
+    rt = bb - op_true(x)
+    rel = np.sqrt(float(rt @ rt) / bn2)
+    if rel <= rtol:
+        return x, 0, rel
+    r = rt.astype(f32)
+    inc = np.zeros_like(r)
+
+    def prec(v):
+        return vcycle(levels, v.reshape(H, W).astype(np.float64), 0, omega, scale).ravel().astype(f32)
+
+    z = prec(r)
+    p = z.copy()
+    rz = float(r.astype(np.float64) @ z)
+    for it in range(1, maxit + 1):
+        q = apply32(p).astype(f32)
+        al = rz / float(p.astype(np.float64) @ q)
+        inc = (inc + f32(al) * p).astype(f32)
+        r = (r - f32(al) * q).astype(f32)
+        rr = float(r.astype(np.float64) @ r)
+        restart = False
+        if it % replace_every == 0 or rr <= rtol * rtol * bn2 or it == maxit:
+            x += inc
+            inc[:] = 0
+            rt = bb - op_true(x)
+            rrt = float(rt @ rt)
+            rel = np.sqrt(rrt / bn2)
+            if rel <= rtol or it == maxit:
+                return x, it, rel
+            restart = restart_gap and rrt > 4.0 * rr
+            r = rt.astype(f32)
+        z = prec(r)
+        rz1 = float(r.astype(np.float64) @ z)
+        p = (z + f32(0.0 if restart else rz1 / rz) * p).astype(f32)
+        rz = rz1
+    return x, maxit, rel

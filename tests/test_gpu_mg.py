@@ -7,7 +7,7 @@ unfinished aggregation operators (gridoperators.h:18-138)."""
 import numpy as np
 import pytest
 
-from gpu_util import oracle_problem, torch_cuda
+from gpu_util import edge_image, oracle_problem, torch_cuda
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-4
@@ -163,24 +163,6 @@ def test_mg_adjoint_matches_cg_adjoint(orc):
         assert np.linalg.norm(a_ - b_) <= 1e-4 * np.linalg.norm(b_)
 
 
-def _edge_image(W, H, seed=0):
-    """RGB8 soft edge with +-4 noise and column strokes (the problem of
-    tests/c/test_native.c)."""
-    v, u = np.mgrid[0:H, 0:W]
-    a = 1.0 / (1.0 + np.exp(-(u - W // 2 + 5.0 * np.sin(v * 0.17 + seed)) / 2.0))
-    i = (u + v * W).astype(np.int64)
-    fg, bg = np.array([230.0, 60.0, 30.0]), np.array([25.0, 80.0, 200.0])
-    img = np.empty((H, W, 3), np.uint8)
-    for c in range(3):
-        n = ((i * 7919 + c * 104729 + seed * 31) % 2**32) % 9 - 4
-        val = a * fg[c] + (1 - a) * bg[c] + n
-        img[..., c] = np.clip(np.floor(val + 0.5), 0, 255).astype(np.uint8)
-    sc = np.full((H, W), 128, np.uint8)
-    sc[(u >= W - 6) & (u < W - 2) & (v % 3 != 0)] = 255
-    sc[(u >= 2) & (u < 6) & (v % 3 != 1)] = 0
-    return img, sc
-
-
 def test_mg_constant_rhs_from_zero_guess(orc):
     """The adjoint of loss = sum(alpha) solves A lambda = 1/2 from lambda = 0.
     lambda reaches ~190 there, so the first 50 iterations carry it all in the
@@ -191,7 +173,7 @@ def test_mg_constant_rhs_from_zero_guess(orc):
     from gpumatting_b200 import api
 
     W, H = 96, 64
-    img, sc = _edge_image(W, H)
+    img, sc = edge_image(W, H)
     st = api.LevinStore(W, H, "fp16").assemble(torch.from_numpy(img).cuda(), torch.from_numpy(sc).cuda(), eps=1e-5,
                                                gamma_value=100.0)
     rhs = torch.full((H, W), 0.5, device="cuda")

@@ -93,3 +93,53 @@ def test_level_shapes_reject_bad_sizes():
     n = C.c_int(0)
     assert L.load().gm_levin_mg_levels(0, 5, C.byref(n), None, 0) == L.GM_ERR_INVALID
     assert L.load().gm_levin_mg_levels(5, -1, C.byref(n), None, 0) == L.GM_ERR_INVALID
+
+
+def test_fp32_scheme_needs_the_restart_rule(orc):
+    """The GPU solver's arithmetic scheme (oracle mg.mgpcg_fp32: FP32 vectors
+    and increment, FP64 replacement every 50) on A lambda = 1/2 from
+    lambda = 0, the adjoint of sum(alpha) on the 96x64 edge image of
+    tests/c/test_native.c.  lambda reaches ~190, so the first 50 iterations
+    carry all of it in the FP32 increment and the first true residual is far
+    above the recurrence's.  Without the gap restart the next beta lets the
+    stale direction swamp the new one and the solve stalls; with it the
+    solve converges in about the FP64 PCG's iterations."""
+    from gpu_util import edge_image
+    from oracle import mg as M
+
+    W, H = 96, 64
+    img, sc = edge_image(W, H)
+    w = np.asarray(orc.levin_sym64(img.astype(np.float64) / 255.0, 1e-5)).reshape(12, -1)
+    g = np.where(sc != 128, 100.0, 0.0).ravel()
+    offs = M.fine_offsets()
+
+    def diag(wp):
+        d = g.reshape(H, W).copy()
+        for k, (du, dv) in enumerate(offs):
+            wk = wp[k].astype(np.float64).reshape(H, W)
+            d += wk + M._shift(wk, -du, -dv)
+        return d.ravel()
+
+    # V-cycle on FP16 planes, outer operator on FP32 planes (the GPU's split)
+    w16 = w.astype(np.float16).astype(np.float64)
+    lv = M.hierarchy(w16, diag(w16), g, W, H)
+    w32 = w.astype(np.float32)
+    d32 = diag(w32).astype(np.float32).reshape(H, W)
+
+    def apply32(x):
+        x = x.reshape(H, W).astype(np.float32)
+        y = d32 * x
+        for k, (du, dv) in enumerate(offs):
+            c = w32[k].reshape(H, W)
+            y = y - c * M._shift(x, du, dv) - M._shift(c * x, -du, -dv)
+        return y.ravel()
+
+    op = orc.Operator(W=W, H=H, w=w32.astype(np.float64), gamma=g)
+    b = np.full(W * H, 0.5)
+    x64, it64, rel64 = M.mgpcg(lv, op.apply, b, np.zeros(W * H), rtol=1e-6, maxit=300)
+    assert rel64 <= 1e-6 and np.abs(x64).max() > 100.0
+    _, it_no, rel_no = M.mgpcg_fp32(lv, op.apply, apply32, b, np.zeros(W * H), rtol=1e-6, maxit=300,
+                                    restart_gap=False)
+    assert rel_no > 1e-5, (it_no, rel_no)  # stalled
+    _, it_yes, rel_yes = M.mgpcg_fp32(lv, op.apply, apply32, b, np.zeros(W * H), rtol=1e-6, maxit=300)
+    assert rel_yes <= 1e-6 and it_yes <= 1.3 * it64 + 10, (it_yes, it64)

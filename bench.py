@@ -54,13 +54,24 @@ REPLACE_BYTES = {"sym_mixed": 92, "ref25": 124}
 IMPORT_BYTES = {"sym_mixed": 36, "ref25": 20}
 
 
-def load_peaks():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        d["source"] = "measured"
-        return d
-    return dict(FALLBACK_PEAKS)
+def load_peaks(path: str | None = None):
+    """The HBM roofline denominator: `hbm_gbs` of the per-pod measured-peaks
+    file when it holds a positive number there, else the fallback (the
+    reason kept in `source`)."""
+    p = path or os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if not os.path.exists(p):
+        return dict(FALLBACK_PEAKS)
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        v = float(d["hbm_gbs"])
+    except (OSError, ValueError, TypeError, KeyError) as e:
+        return dict(FALLBACK_PEAKS, source=f"fallback ({os.path.basename(p)} unreadable: {type(e).__name__})")
+    if not v > 0.0:
+        return dict(FALLBACK_PEAKS, source=f"fallback ({os.path.basename(p)} hbm_gbs = {v})")
+    d["hbm_gbs"] = v
+    d["source"] = "measured"
+    return d
 
 
 class ClockSampler:

@@ -1,0 +1,41 @@
+"""Host-side pieces of bench.py that need no GPU: the roofline denominator
+read from the per-pod measured-peaks file, with the fallback and its reason
+when the file is absent or does not hold a usable `hbm_gbs`."""
+import importlib.util
+import json
+import os
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_load_peaks_measured_and_fallbacks(tmp_path):
+    B = _bench()
+    absent = B.load_peaks(str(tmp_path / "none.json"))
+    assert absent == B.FALLBACK_PEAKS and absent["source"] == "fallback"
+
+    good = tmp_path / "good.json"
+    good.write_text(json.dumps({"hbm_gbs": "6557.2", "bf16_tflops": 1590.0}))
+    d = B.load_peaks(str(good))
+    assert d["hbm_gbs"] == 6557.2 and d["source"] == "measured" and d["bf16_tflops"] == 1590.0
+
+    for name, text, why in (("nokey.json", json.dumps({"bf16_tflops": 1.0}), "KeyError"),
+                            ("bad.json", "{not json", "JSONDecodeError"),
+                            ("nan.json", json.dumps({"hbm_gbs": "fast"}), "ValueError"),
+                            ("null.json", json.dumps({"hbm_gbs": None}), "TypeError")):
+        f = tmp_path / name
+        f.write_text(text)
+        d = B.load_peaks(str(f))
+        assert d["hbm_gbs"] == B.FALLBACK_PEAKS["hbm_gbs"], name
+        assert d["source"].startswith("fallback") and why in d["source"], d["source"]
+
+    zero = tmp_path / "zero.json"
+    zero.write_text(json.dumps({"hbm_gbs": 0}))
+    d = B.load_peaks(str(zero))
+    assert d["hbm_gbs"] == B.FALLBACK_PEAKS["hbm_gbs"] and "hbm_gbs = 0" in d["source"]

@@ -485,13 +485,13 @@ def run_ours(args):
             pl["speedup_mixed_mg_step_vs_plain_solve"] = pl["ms_per_solve"] / line["mg"]["ms_per_step"]
         line["plain_fp32"] = pl
     if rank == 0 and world == 1 and not args.no_solvers:
-        line["solvers"] = run_solvers(args, prob, img_d, scr_d, store, flush, stream)
+        line["solvers"] = supplementary("solvers", lambda: run_solvers(args, prob, img_d, scr_d, store, flush, stream))
     if args.batch_count > 0:
         line["batch"] = run_batch(args, stream, world, rank)
     if rank == 0 and world == 1 and args.large_size > 0:
-        line["large"] = run_large(args, stream, peaks)
+        line["large"] = supplementary("large", lambda: run_large(args, stream, peaks))
     if rank == 0 and world == 1 and args.spmv_size > 0:
-        line["spmv"] = run_spmv(args, stream, peaks)
+        line["spmv"] = supplementary("spmv", lambda: run_spmv(args, stream, peaks))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sweeps = calibrate_sweeps(prob, args.cpu_seconds)
         times, kind, asm = reference_cpu_path(prob, sweeps, 1, steps=1)
@@ -530,6 +530,18 @@ def cached_problem(W: int, H: int, seed: int):
     if key not in _PROBLEMS:
         _PROBLEMS[key] = make_problem(W, H, seed)
     return _PROBLEMS[key]
+
+
+def supplementary(name: str, fn) -> dict:
+    """Runs one single-rank section after the headline numbers exist; a
+    failure there is reported in its own key instead of losing the line."""
+    import traceback
+
+    try:
+        return fn()
+    except Exception as e:  # noqa: BLE001 - any failure of an extra section
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{type(e).__name__}: {e}"[:300], "section": name}
 
 
 def run_large(args, stream, peaks) -> dict:

@@ -39,3 +39,14 @@ def test_load_peaks_measured_and_fallbacks(tmp_path):
     zero.write_text(json.dumps({"hbm_gbs": 0}))
     d = B.load_peaks(str(zero))
     assert d["hbm_gbs"] == B.FALLBACK_PEAKS["hbm_gbs"] and "hbm_gbs = 0" in d["source"]
+
+
+def test_supplementary_section_failure_keeps_the_line():
+    B = _bench()
+    assert B.supplementary("ok", lambda: {"x": 1}) == {"x": 1}
+
+    def boom():
+        raise RuntimeError("out of memory at 4096^2")
+
+    d = B.supplementary("large", boom)
+    assert d["section"] == "large" and d["error"].startswith("RuntimeError: out of memory")

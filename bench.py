@@ -464,11 +464,12 @@ def run_ours(args):
         ms32, res32 = timed_solve("mg", args.steps, use_low=0)
         line["mg"]["fp32_planes"] = {"solve_only_ms": ms32, "iters": res32[0].iters,
                                      "rel_residual": res32[0].rel_residual}
-        # algorithmic bytes per pixel-iteration (FP16 V-cycle planes, FP32 outer operator)
-        mg_bytes = N * MG_BYTES_PER_PX_ITER * (it_m / args.steps)
+        # algorithmic bytes per pixel-iteration of the store's precision
+        mg_bpp = MG_BYTES_PER_PX_ITER[args.precision]
+        mg_bytes = N * mg_bpp * (it_m / args.steps)
         mg_gbs = mg_bytes / (line["mg"]["solve_ms"] / 1000.0) / 1e9
         line["mg"]["roofline"] = {"bound": "hbm", "achieved": mg_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                                  "frac": mg_gbs / peaks["hbm_gbs"], "bytes_per_px_iter": MG_BYTES_PER_PX_ITER,
+                                  "frac": mg_gbs / peaks["hbm_gbs"], "bytes_per_px_iter": mg_bpp,
                                   "peak_source": peaks.get("source")}
     if rank == 0 and world == 1 and not args.no_plain:
         # speed-ups on equal footing: solve-only time of each arm, from alpha = 0.5
@@ -507,12 +508,14 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-# Multigrid PCG, algorithmic bytes per pixel-iteration: SpMV 68 (FP32 planes
-# 48, d32, z and p read, p and q written), update 24 (FP32 solution increment
-# read/write, p, q, r read, r written), level-0 restriction 33 and
-# prolongation 37 (FP16 planes 24, r, 1/d, the coarse side, z written),
-# coarse levels 18 (54 B per coarse cell, a third of a pixel).
-MG_BYTES_PER_PX_ITER = 68 + 24 + 33 + 37 + 18
+# Multigrid PCG on an FP16 store, algorithmic bytes per pixel-iteration:
+# SpMV 44 (FP16 planes 24, d, z and p read, p and q written), update 24 (FP32
+# solution increment read/write, p, q, r read, r written), level-0
+# restriction 33 and prolongation 37 (FP16 planes 24, r, 1/d, the coarse
+# side, z written), coarse levels 18 (54 B per coarse cell, a third of a
+# pixel).  A BF16 or FP32 store's SpMV reads the FP32 planes: 68.
+MG_BYTES_PER_PX_ITER = {"fp16": 44 + 24 + 33 + 37 + 18, "bf16": 68 + 24 + 33 + 37 + 18,
+                        "fp32": 68 + 24 + 57 + 61 + 18}  # FP32 planes 48 in restriction / prolongation
 
 # Algorithmic bytes per pixel of one SpMV pass: band planes + diagonal plane
 # + x read once + y written once.

@@ -592,6 +592,15 @@ struct FineLayout {
     static constexpr uint32_t bytes = (uint32_t)(PB + 2 * VB + XB + DB);
 };
 
+// Element type of the planes a level-0 kernel streams: the iteration planes,
+// except that the SpMV of a BF16 store reads the FP32 planes (a BF16 outer
+// operator costs more iterations than its bytes save; FP16 costs few).
+template <int MODE, class T>
+struct FinePlanes {
+    using PT = typename std::conditional<MODE == FM_SPMV && !std::is_same<T, __half>::value, float, T>::type;
+    static constexpr int ES = (int)sizeof(PT);
+};
+
 template <class T> __device__ __forceinline__ float2 ld2(const T* p);
 template <> __device__ __forceinline__ float2 ld2<float>(const float* p) { return *reinterpret_cast<const float2*>(p); }
 template <> __device__ __forceinline__ float2 ld2<__half>(const __half* p)
@@ -633,11 +642,11 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, State
 }
 
 template <int MODE, class S, class T>
-__global__ void __launch_bounds__(FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T), S::NP>::THR, 1)
+__global__ void __launch_bounds__(FineLayout<MODE, FinePlanes<MODE, T>::ES, S::NP>::THR, 1)
     mg_fine_kernel(const __grid_constant__ TMaps tm, Args a, int l)
 {
-    constexpr int ES = MODE == FM_SPMV ? 4 : (int)sizeof(T);
-    using PT = typename std::conditional<MODE == FM_SPMV, float, T>::type;
+    constexpr int ES = FinePlanes<MODE, T>::ES;
+    using PT = typename FinePlanes<MODE, T>::PT;
     using LY = FineLayout<MODE, ES, S::NP>;
     constexpr int TH = LY::TH, NT = LY::THR, RPT = TH / (NT / 64);
     static_assert(RPT == 2, "each thread covers one row pair");
@@ -1245,11 +1254,16 @@ static int make_maps(const Args& a, int es, CUtensorMapDataType dt, FineMaps& fm
     };
     const int t32 = fine_rows(4), tlo = fine_rows(es);
     const Lev& L0 = a.lev[0];
-    GM_TRY(planes(&fm.spmv.m[0], a.w32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.ps32, t32));
-    GM_TRY(vec(&fm.spmv.m[1], L0.x, W, H, P, kFBW, t32 + 4));
-    GM_TRY(vec(&fm.spmv.m[2], a.p0, W, H, P, kFBW, t32 + 4));
-    GM_TRY(vec(&fm.spmv.m[3], a.p1, W, H, P, kFBW, t32 + 4));
-    GM_TRY(vec(&fm.spmv.m[4], a.d32, W, H, P, kFTW, t32));
+    // the SpMV streams the FP16 iteration planes and their diagonal d when
+    // the iterations run on FP16 planes, else the FP32 planes and d32
+    const bool lo16 = es == 2 && dt == CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const int ts = lo16 ? tlo : t32;
+    if (lo16) GM_TRY(planes(&fm.spmv.m[0], L0.c, dt, 2, L0.ps, ts));
+    else GM_TRY(planes(&fm.spmv.m[0], a.w32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.ps32, ts));
+    GM_TRY(vec(&fm.spmv.m[1], L0.x, W, H, P, kFBW, ts + 4));
+    GM_TRY(vec(&fm.spmv.m[2], a.p0, W, H, P, kFBW, ts + 4));
+    GM_TRY(vec(&fm.spmv.m[3], a.p1, W, H, P, kFBW, ts + 4));
+    GM_TRY(vec(&fm.spmv.m[4], lo16 ? L0.D : a.d32, W, H, P, kFTW, ts));
     for (int l = 0; l < a.lt; ++l) {
         // level 0: the store's planes (12, iteration precision); below: 4 FP32 planes
         const Lev& F = a.lev[l];
@@ -1308,7 +1322,7 @@ struct Enq {
         const Lev& F = a.lev[l];
         const TMaps& m = MODE == FM_SPMV ? fm->spmv : (MODE == FM_DOWN ? fm->down[l] : fm->up[l]);
         if (l == 0) {
-            using LY = FineLayout<MODE, MODE == FM_SPMV ? 4 : (int)sizeof(T), 12>;
+            using LY = FineLayout<MODE, FinePlanes<MODE, T>::ES, 12>;
             const int tiles = ((F.W + kFTW - 1) / kFTW) * ((F.H + LY::TH - 1) / LY::TH);
             go(mg_fine_kernel<MODE, FineSten, T>, tiles, LY::total, LY::THR, m, a, 0);
         } else {

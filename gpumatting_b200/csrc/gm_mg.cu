@@ -125,6 +125,8 @@ struct Args {
     State* st;
     double rtol;
     int max_iters, replace_every;
+    int outer_low;  // the level-0 SpMV streams the FP16 iteration planes, not w32
+    int spare;      // keeps the struct free of padding (it is compared bytewise)
     float omega, scale;
     unsigned long long cond;  // conditional-node handle (0 = host-driven loop)
 };
@@ -551,7 +553,8 @@ static int tail_bytes(const int* Wl, const int* Hl, int lt, int L)
 // the image.  After a stage lands, the CTA forms the stencil input in a
 // shared tile, then each thread marches TH / 4 rows of a column pair with a
 // 5 x 6 window of it in registers.
-//   FM_SPMV  input z + beta p_old; q = A p_new with the FP32 planes and d32;
+//   FM_SPMV  input z + beta p_old; q = A p_new with the FP32 planes and d32
+//            (FP16 planes and d when Args::outer_low);
 //            writes p_new and q, sums p_new . q (the last CTA forms alpha).
 //   FM_DOWN  input x1 = omega b / d; rho = b - A x1, summed over 2 x 2 blocks
 //            into the level-1 right-hand side.
@@ -592,9 +595,11 @@ struct FineLayout {
     static constexpr uint32_t bytes = (uint32_t)(PB + 2 * VB + XB + DB);
 };
 
-// Element type of the planes a level-0 kernel streams: the iteration planes,
-// except that the SpMV of a BF16 store reads the FP32 planes (a BF16 outer
-// operator costs more iterations than its bytes save; FP16 costs few).
+// Element type of the planes a level-0 kernel streams: the iteration planes.
+// The SpMV of a BF16 store reads the FP32 planes instead (a BF16 outer
+// operator costs more iterations than its bytes save); so does an FP16
+// store's when the tolerance is tight (Args::outer_low = 0), through the
+// float instantiation.
 template <int MODE, class T>
 struct FinePlanes {
     using PT = typename std::conditional<MODE == FM_SPMV && !std::is_same<T, __half>::value, float, T>::type;
@@ -1235,6 +1240,18 @@ struct FineMaps {
     TMaps spmv, down[kMaxLevels], up[kMaxLevels];
 };
 
+// Whether the outer SpMV streams the FP16 iteration planes (tcode 1) rather
+// than the FP32 ones.  It saves 24 of ~180 B per pixel-iteration, and the
+// FP16 outer operator costs 1 % more iterations at rtol 1e-6 (1080p: 87
+// against 86).  Between replacements each cycle can refine less, so below
+// 1e-7 the extra iterations outweigh it (1e-10: 408 against 331), and the
+// FP32 planes stay.  rtol <= 0 (a fixed iteration count) takes the FP16 ones.
+constexpr double kOuterLowMinRtol = 1e-7;
+static int outer_low_for(int tcode, double rtol)
+{
+    return tcode == 1 && !(rtol > 0.0 && rtol < kOuterLowMinRtol) ? 1 : 0;
+}
+
 // Tensor maps of the level-0 kernels (es: bytes per element of the
 // iteration planes).
 static int make_maps(const Args& a, int es, CUtensorMapDataType dt, FineMaps& fm)
@@ -1255,8 +1272,8 @@ static int make_maps(const Args& a, int es, CUtensorMapDataType dt, FineMaps& fm
     const int t32 = fine_rows(4), tlo = fine_rows(es);
     const Lev& L0 = a.lev[0];
     // the SpMV streams the FP16 iteration planes and their diagonal d when
-    // the iterations run on FP16 planes, else the FP32 planes and d32
-    const bool lo16 = es == 2 && dt == CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    // outer_low is set, else the FP32 planes and d32
+    const bool lo16 = es == 2 && dt == CU_TENSOR_MAP_DATA_TYPE_FLOAT16 && a.outer_low;
     const int ts = lo16 ? tlo : t32;
     if (lo16) GM_TRY(planes(&fm.spmv.m[0], L0.c, dt, 2, L0.ps, ts));
     else GM_TRY(planes(&fm.spmv.m[0], a.w32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.ps32, ts));
@@ -1321,7 +1338,11 @@ struct Enq {
     {
         const Lev& F = a.lev[l];
         const TMaps& m = MODE == FM_SPMV ? fm->spmv : (MODE == FM_DOWN ? fm->down[l] : fm->up[l]);
-        if (l == 0) {
+        if (l == 0 && MODE == FM_SPMV && !a.outer_low) {
+            using LY = FineLayout<MODE, 4, 12>;
+            const int tiles = ((F.W + kFTW - 1) / kFTW) * ((F.H + LY::TH - 1) / LY::TH);
+            go(mg_fine_kernel<MODE, FineSten, float>, tiles, LY::total, LY::THR, m, a, 0);
+        } else if (l == 0) {
             using LY = FineLayout<MODE, FinePlanes<MODE, T>::ES, 12>;
             const int tiles = ((F.W + kFTW - 1) / kFTW) * ((F.H + LY::TH - 1) / LY::TH);
             go(mg_fine_kernel<MODE, FineSten, T>, tiles, LY::total, LY::THR, m, a, 0);
@@ -1653,6 +1674,7 @@ int run_mg_solver(const gm_levin_store* store, const float* b, int bpitch, const
     a.alpha_in = alpha_in;
     a.alpha_out = alpha_out;
     a.rtol = p->rtol;
+    a.outer_low = outer_low_for(tcode, a.rtol);
     a.max_iters = p->max_iters;
     a.replace_every = p->replace_every;
     a.omega = p->mg_omega > 0.f ? p->mg_omega : kDefaultOmega;
@@ -1767,6 +1789,7 @@ extern "C" int gm_levin_solve_mg_many(const gm_levin_store* const* stores, float
         a.alpha_in = alphas[k];
         a.alpha_out = alphas[k];
         a.rtol = p.rtol;
+        a.outer_low = outer_low_for(tcode, a.rtol);
         a.max_iters = p.max_iters;
         a.replace_every = p.replace_every;
         a.omega = p.mg_omega > 0.f ? p.mg_omega : kDefaultOmega;

@@ -168,7 +168,10 @@ enum { GM_PREC_FP32 = 0, GM_PREC_FP16 = 1, GM_PREC_BF16 = 2 };
  * Jacobi step before and after each coarse correction, exact solve of the
  * coarsest level of <= 128 cells); symmetric stores (gm_levin_solve,
  * gm_levin_solve_rhs, gm_levin_adjoint, gm_levin_solve_mg_many) and batches
- * (gm_batch_solve, one graph launch per image).  The reference
+ * (gm_batch_solve, one graph launch per image).  The outer matrix products
+ * read the FP16 planes of an FP16 store when rtol >= 1e-7 (or <= 0), else the
+ * FP32 planes; convergence is always judged on the FP32 operator's FP64
+ * residual.  The reference
  * sketches aggregation operators over superpixels for this purpose
  * (gridoperators.h:18-138, SLIC.cpp:32, commented out at main.cu:201-218)
  * without finishing them. */

@@ -143,3 +143,54 @@ def test_fp32_scheme_needs_the_restart_rule(orc):
     assert rel_no > 1e-5, (it_no, rel_no)  # stalled
     _, it_yes, rel_yes = M.mgpcg_fp32(lv, op.apply, apply32, b, np.zeros(W * H), rtol=1e-6, maxit=300)
     assert rel_yes <= 1e-6 and it_yes <= 1.3 * it64 + 10, (it_yes, it64)
+
+
+def test_fp16_outer_operator_pays_only_at_loose_tolerance(orc):
+    """The GPU solver takes the FP16 planes for the outer matrix products of
+    an FP16 store only when rtol >= 1e-7.  In its FP32 scheme (oracle
+    mg.mgpcg_fp32) the FP16 outer operator costs a few iterations at 1e-6
+    but many at 1e-10: between replacements each cycle can only refine as
+    far as the FP16 operator allows."""
+    from oracle import mg as M
+
+    W, H = 240, 160
+    p = make_problem(W, H, 0)
+    w = np.asarray(orc.levin_sym64(p.image.astype(np.float64) / 255.0, p.eps)).reshape(12, -1)
+    g = p.gamma.ravel().astype(np.float64)
+    b = (p.gamma * p.s).ravel().astype(np.float64)
+    offs = M.fine_offsets()
+
+    def diag(wp):
+        d = g.reshape(H, W).copy()
+        for k, (du, dv) in enumerate(offs):
+            wk = wp[k].astype(np.float64).reshape(H, W)
+            d += wk + M._shift(wk, -du, -dv)
+        return d.ravel()
+
+    def operator32(wp):
+        dp = diag(wp).astype(np.float32).reshape(H, W)
+
+        def apply(x):
+            x = x.reshape(H, W).astype(np.float32)
+            y = dp * x
+            for k, (du, dv) in enumerate(offs):
+                c = wp[k].reshape(H, W)
+                y = y - c * M._shift(x, du, dv) - M._shift(c * x, -du, -dv)
+            return y.ravel()
+
+        return apply
+
+    w16 = w.astype(np.float16).astype(np.float32)
+    w32 = w.astype(np.float32)
+    lv = M.hierarchy(w16.astype(np.float64), diag(w16), g, W, H)
+    op = orc.Operator(W=W, H=H, w=w32.astype(np.float64), gamma=g)
+    it = {}
+    for rtol in (1e-6, 1e-10):
+        for name, wp in (("fp32", w32), ("fp16", w16)):
+            _, n, rel = M.mgpcg_fp32(lv, op.apply, operator32(wp), b, np.full(W * H, 0.5), rtol=rtol, maxit=2000)
+            assert rel <= rtol, (name, rtol, n, rel)  # both converge on the true operator
+            it[name, rtol] = n
+    loose = it["fp16", 1e-6] / it["fp32", 1e-6]
+    tight = it["fp16", 1e-10] / it["fp32", 1e-10]
+    assert loose <= 1.1, it
+    assert tight >= loose + 0.15, it

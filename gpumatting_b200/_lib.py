@@ -87,6 +87,7 @@ SIGNATURES = {
     "hostLevinLaplacian": (None, [BandedMatrix, _vp, _f, _vp, _vp, _i, _i, _sz]),
     "gaussSeidel_host": (None, [_vp, C.POINTER(BandedMatrix), _vp, _sz]),
     "jacobi_host": (None, [_vp, C.POINTER(BandedMatrix), _vp, _sz, _i, _f]),
+    "gm_gs_host_levels": (_i, [C.POINTER(BandedMatrix)]),
     "computeError": (None, [_vp, _vp, _i, _i]),
     "gm_bm_ax": (_i, [_vp, BandedMatrix, _vp, _vp]),
     "gm_bm_axpy": (_i, [_vp, BandedMatrix, _vp, _vp, _i, _vp]),

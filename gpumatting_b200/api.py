@@ -133,13 +133,29 @@ def hostLevinLaplacian(bands_host: np.ndarray, b_host: np.ndarray, lam: float, i
     L.check(lib.gm_last_status())
 
 
-def jacobi_host(x_padded: np.ndarray, pad: int, bands_host: np.ndarray, offsets, b: np.ndarray, iterations: int,
-                omega: float = 2.0 / 3.0):
-    """Solve.cpp:35-85 semantics on host arrays (x_padded has `pad` zeros each side)."""
-    lib = L.load()
+def _host_matrix(bands_host: np.ndarray, offsets, x_padded: np.ndarray, pad: int):
+    """BandedMatrix view of host bands (nbands, N) + checks that x_padded is a
+    float32 vector with `pad` >= max |offset| elements either side, since the
+    library reads x as far as the pattern reaches."""
     offs = np.ascontiguousarray(offsets, np.int32)
     a = np.ascontiguousarray(bands_host, np.float32)
-    m = L.BandedMatrix(a.ctypes.data, a.shape[1], offs.ctypes.data, a.shape[0], a.shape[1], a.shape[1])
+    if a.ndim != 2 or a.shape[0] != offs.size:
+        raise ValueError("bands_host must be (nbands, N) with one offset per band")
+    n = a.shape[1]
+    if x_padded.dtype != np.float32 or not x_padded.flags.c_contiguous or x_padded.size != n + 2 * pad:
+        raise ValueError(f"x_padded must be contiguous float32 of N + 2*pad = {n + 2 * pad} elements")
+    if offs.size and pad < int(np.abs(offs).max()):
+        raise ValueError(f"pad {pad} is smaller than the band reach {int(np.abs(offs).max())}")
+    m = L.BandedMatrix(a.ctypes.data, n, offs.ctypes.data, a.shape[0], n, n)
+    return m, (a, offs)
+
+
+def jacobi_host(x_padded: np.ndarray, pad: int, bands_host: np.ndarray, offsets, b: np.ndarray, iterations: int,
+                omega: float = 2.0 / 3.0):
+    """Solve.cpp:35-85 on host arrays (x_padded has `pad` elements each side);
+    the iterates are bit-identical to the reference's."""
+    lib = L.load()
+    m, keep = _host_matrix(bands_host, offsets, x_padded, pad)
     bb = np.ascontiguousarray(b, np.float32)
     lib.jacobi_host(x_padded.ctypes.data + 4 * pad, C.byref(m), bb.ctypes.data, iterations, pad, omega)
     L.check(lib.gm_last_status())
@@ -147,13 +163,22 @@ def jacobi_host(x_padded: np.ndarray, pad: int, bands_host: np.ndarray, offsets,
 
 def gaussSeidel_host(x_padded: np.ndarray, pad: int, bands_host: np.ndarray, offsets, b: np.ndarray,
                      iterations: int):
+    """Solve.cpp:3-33 on host arrays, any band pattern; bit-identical to the
+    reference's sequential sweep."""
     lib = L.load()
-    offs = np.ascontiguousarray(offsets, np.int32)
-    a = np.ascontiguousarray(bands_host, np.float32)
-    m = L.BandedMatrix(a.ctypes.data, a.shape[1], offs.ctypes.data, a.shape[0], a.shape[1], a.shape[1])
+    m, keep = _host_matrix(bands_host, offsets, x_padded, pad)
     bb = np.ascontiguousarray(b, np.float32)
     lib.gaussSeidel_host(x_padded.ctypes.data + 4 * pad, C.byref(m), bb.ctypes.data, iterations)
     L.check(lib.gm_last_status())
+
+
+def gs_host_levels(bands_host: np.ndarray, offsets) -> int:
+    """Levels of gaussSeidel_host's schedule (dependent steps per sweep)."""
+    offs = np.ascontiguousarray(offsets, np.int32)
+    a = np.ascontiguousarray(bands_host, np.float32)
+    n = a.shape[1]
+    m = L.BandedMatrix(a.ctypes.data, n, offs.ctypes.data, a.shape[0], n, n)
+    return int(L.load().gm_gs_host_levels(C.byref(m)))
 
 
 # ---------------------------------------------------------------------------
@@ -171,8 +196,25 @@ def jacobi_step(xx, x: PaddedVector, Lm: DeviceBandedMatrix, b, omega: float, st
     L.check(L.load().gm_jacobi_step(_ptr(xx), x.ptr, Lm.struct, _ptr(b), omega, _stream(stream)))
 
 
+def _check_dot_operands(x, y):
+    torch = _torch()
+    if not (isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor)):
+        raise TypeError("x and y must be torch tensors")
+    if x.dtype != torch.float32 or y.dtype != torch.float32:
+        raise TypeError(f"x and y must be float32 (got {x.dtype}, {y.dtype})")
+    if not (x.is_cuda and y.is_cuda) or x.device != y.device:
+        raise ValueError("x and y must be CUDA tensors on one device")
+    if not (x.is_contiguous() and y.is_contiguous()):
+        raise ValueError("x and y must be contiguous")
+    if x.numel() != y.numel():
+        raise ValueError(f"x and y differ in length ({x.numel()} vs {y.numel()})")
+    if x.numel() > 2**31 - 1:
+        raise ValueError("vectors longer than 2^31 - 1 elements are not supported")
+
+
 def inner_prod(x, y, stream=None, f64: bool = False):
     torch = _torch()
+    _check_dot_operands(x, y)
     out = torch.zeros(1, dtype=torch.float64 if f64 else torch.float32, device=x.device)
     fn = L.load().gm_inner_prod_f64 if f64 else L.load().gm_inner_prod
     L.check(fn(out.data_ptr(), x.data_ptr(), y.data_ptr(), x.numel(), _stream(stream)))
@@ -180,7 +222,19 @@ def inner_prod(x, y, stream=None, f64: bool = False):
 
 
 def inner_prod_noalloc(x, y, out, stream=None):
-    """<x, y> in FP64 into the device double `out`, allocating nothing."""
+    """<x, y> in FP64 into the device double `out`, allocating nothing.
+
+    `out` must be a float64 CUDA tensor on the operands' device: the library
+    writes one 8-byte double there, so a float32 or host tensor is refused
+    here rather than overrun on the device."""
+    torch = _torch()
+    _check_dot_operands(x, y)
+    if not isinstance(out, torch.Tensor) or out.dtype != torch.float64 or not out.is_cuda or out.numel() < 1:
+        raise TypeError("out must be a float64 CUDA tensor with at least one element")
+    if out.device != x.device:
+        raise ValueError("out must be on the operands' device")
+    if not out.is_contiguous():
+        raise ValueError("out must be contiguous")
     L.check(L.load().gm_inner_prod_f64_noalloc(out.data_ptr(), x.data_ptr(), y.data_ptr(), x.numel(),
                                                _stream(stream)))
     return out

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpumat.so")
-SOURCES = ["gm_common.cu", "gm_vector.cu", "gm_banded.cu", "gm_levin.cu", "gm_apply.cu", "gm_io.cu", "gm_solver.cu", "gm_mg.cu", "gm_capi.cu"]
+SOURCES = ["gm_common.cu", "gm_vector.cu", "gm_banded.cu", "gm_levin.cu", "gm_apply.cu", "gm_io.cu", "gm_solver.cu", "gm_mg.cu", "gm_capi.cu", "gm_hostsolve.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -27,30 +27,6 @@ static bool levin_pattern(const int* offs, int nb, int rows, int* W_out)
     return true;
 }
 
-// 9-colour Gauss-Seidel sweep on the Levin stencil: pixels with
-// (u mod 3, v mod 3) == colour never neighbour each other in the 5x5
-// stencil, so one colour updates in parallel with the same arithmetic as
-// Solve.cpp:16-31 (middle band skipped, then divided by it).
-__global__ void gs_colour_kernel(float* x, const float* __restrict__ a, size_t apitch, const int* __restrict__ bands,
-                                 int nbands, int W, int H, const float* __restrict__ b, int cu, int cv)
-{
-    __shared__ int off[32];
-    for (int j = threadIdx.x; j < nbands; j += blockDim.x) off[j] = bands[j];
-    __syncthreads();
-    const int nu = (W - cu + 2) / 3, nv = (H - cv + 2) / 3;
-    const int mid = nbands / 2;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nu * nv; t += gridDim.x * blockDim.x) {
-        const int u = cu + 3 * (t % nu), v = cv + 3 * (t / nu);
-        const size_t i = (size_t)v * W + u;
-        float s = 0.f;
-        for (int j = 0; j < nbands; ++j) {
-            if (j == mid) continue;
-            s += a[i + (size_t)j * apitch] * x[(long long)i + off[j]];
-        }
-        x[i] = (b[i] - s) / a[i + (size_t)mid * apitch];
-    }
-}
-
 }  // namespace gm
 
 using namespace gm;
@@ -301,94 +277,5 @@ extern "C" void hostLevinLaplacian(BandedMatrix L, float* b, float lambda, gm_fl
     cudaFree(dsc);
     cudaFree(da);
     cudaFree(db);
-    gm_note_status(rc);
-}
-
-// Host BandedMatrix -> device copy helper for the *_host drop-ins.
-static int host_to_device(const BandedMatrix* A, BandedMatrix* dA)
-{
-    bmCopyToDevice(dA, A);
-    return gm_last_status();
-}
-
-// Solve.cpp:35-85 on the GPU.  The reference's diagonal is band nbands/2;
-// the Levin store (and every pattern this accepts) keeps offset 0 there.
-extern "C" void jacobi_host(float* x, const BandedMatrix* A, const float* b, size_t iterations, int xpad,
-                            float omega)
-{
-    if (!x || !A || !b || xpad < 0) { gm_set_error_msg("jacobi_host: bad arguments"); gm_note_status(GM_ERR_INVALID); return; }
-    const int n = A->rows;
-    if (A->nbands <= 0 || A->bands[A->nbands / 2] != 0) {
-        gm_set_error_msg("jacobi_host: the middle band must be the diagonal");
-        gm_note_status(GM_ERR_INVALID);
-        return;
-    }
-    BandedMatrix dA;
-    int rc = host_to_device(A, &dA);
-    float* dx = nullptr;
-    float* dbv = nullptr;
-    if (rc == GM_OK) {
-        vecDeviceMalloc(&dx, n, xpad, xpad);
-        rc = gm_last_status();
-    }
-    if (rc == GM_OK && (cudaMalloc((void**)&dbv, sizeof(float) * (n > 0 ? n : 1)) != cudaSuccess)) rc = GM_ERR_NOMEM;
-    if (rc == GM_OK && (cudaMemcpy(dx, x, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-                        cudaMemcpy(dbv, b, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess))
-        rc = GM_ERR_CUDA;
-    if (rc == GM_OK) {
-        gm_solve_params p;
-        gm_default_params(&p);
-        p.solver = GM_SOLVER_JACOBI;
-        p.rtol = 0.0;
-        p.max_iters = (int)iterations;
-        p.omega = omega;
-        gm_solve_info info;
-        rc = gm_banded_solve(dA, 0, dx, xpad, dbv, &p, &info, nullptr);
-        if (rc == GM_OK && cudaMemcpy(x, dx, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) rc = GM_ERR_CUDA;
-    }
-    if (dx) vecDeviceFree(dx, xpad);
-    if (dbv) cudaFree(dbv);
-    bmDeviceFree(&dA);
-    gm_note_status(rc);
-}
-
-// Solve.cpp:3-33 on the GPU as 9-colour Gauss-Seidel (Levin stencil only).
-extern "C" void gaussSeidel_host(float* x, const BandedMatrix* A, const float* b, size_t iterations)
-{
-    if (!x || !A || !b) { gm_set_error_msg("gaussSeidel_host: bad arguments"); gm_note_status(GM_ERR_INVALID); return; }
-    int W = 0;
-    if (!levin_pattern(A->bands, A->nbands, A->rows, &W)) {
-        gm_set_error_msg("gaussSeidel_host: only the 25-band Levin stencil is supported");
-        gm_note_status(GM_ERR_UNSUPPORTED);
-        return;
-    }
-    const int n = A->rows, H = n / W;
-    const int pad = 2 * W + 2;
-    BandedMatrix dA;
-    int rc = host_to_device(A, &dA);
-    float* dx = nullptr;
-    float* dbv = nullptr;
-    if (rc == GM_OK) {
-        vecDeviceMalloc(&dx, n, pad, pad);
-        rc = gm_last_status();
-    }
-    if (rc == GM_OK && cudaMalloc((void**)&dbv, sizeof(float) * n) != cudaSuccess) rc = GM_ERR_NOMEM;
-    if (rc == GM_OK && (cudaMemcpy(dx, x, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-                        cudaMemcpy(dbv, b, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess))
-        rc = GM_ERR_CUDA;
-    if (rc == GM_OK) {
-        for (size_t it = 0; it < iterations; ++it)
-            for (int c = 0; c < 9; ++c) {
-                const int cu = c % 3, cv = c / 3;
-                const int cnt = ((W - cu + 2) / 3) * ((H - cv + 2) / 3);
-                const int nb = std::max(1, std::min((cnt + 255) / 256, 148 * 4));
-                gs_colour_kernel<<<nb, 256>>>(dx, dA.a, dA.apitch, dA.bands, 25, W, H, dbv, cu, cv);
-            }
-        if (cudaGetLastError() != cudaSuccess) rc = GM_ERR_CUDA;
-        if (rc == GM_OK && cudaMemcpy(x, dx, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) rc = GM_ERR_CUDA;
-    }
-    if (dx) vecDeviceFree(dx, pad);
-    if (dbv) cudaFree(dbv);
-    bmDeviceFree(&dA);
     gm_note_status(rc);
 }

@@ -5,6 +5,8 @@
 // blocks race on zeroing the result while others add into it: here every
 // block writes an FP64 partial and a single-warp pass adds them in block
 // order, so the result is deterministic and exact to FP64 rounding.
+#include <climits>
+
 #include "gm_internal.cuh"
 
 int gm_note_status(int s);
@@ -17,15 +19,19 @@ __global__ void vec_axpby_kernel(float* __restrict__ out, const float* __restric
                                  float a, float b, const float* __restrict__ dev_scale, int n)
 {
     const float s = dev_scale ? *dev_scale : a;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         out[i] = y ? s * x[i] + b * y[i] : s * x[i];
 }
 
+// Grid-stride loops index with 64 bits: n may come within one stride of
+// INT_MAX, where a 32-bit i + stride would overflow.
 __global__ void dot_partial_kernel(const float* __restrict__ x, const float* __restrict__ y, int n, double* part)
 {
     __shared__ double red[32];
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         acc[0] += (double)x[i] * (double)y[i];
     block_sum<1>(acc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
@@ -46,7 +52,8 @@ __global__ void mse_partial_kernel(const float* __restrict__ a, const float* __r
 {
     __shared__ double red[32];
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float av = a[i], gv = g[i];
         float d;
         if (av > 1.0f) d = 1.0f - gv;       // main.cu:567-572
@@ -135,6 +142,10 @@ extern "C" int gm_inner_prod_f64(double* result, const float* x, const float* y,
 extern "C" int gm_compute_error(double* mse_host, const float* alpha, const float* gt, int W, int H, void* stream)
 {
     if (!mse_host || !alpha || !gt || W <= 0 || H <= 0) { gm_set_error_msg("bad compute_error arguments"); return GM_ERR_INVALID; }
+    if ((long long)W * H > INT_MAX) {
+        gm_set_error_msg("compute_error: W*H = %lld exceeds INT_MAX", (long long)W * H);
+        return GM_ERR_INVALID;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     const int n = W * H;
     const int nb = dot_blocks(n);
@@ -221,20 +232,56 @@ __device__ __align__(256) double g_static_dot_parts[kStaticDotParts];
 
 #include <mutex>
 
+// The driver's identifier of the current context (unique for the life of
+// the process, never reused), or 0 when the driver cannot say.
+static unsigned long long current_context_id()
+{
+    typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+    typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrentFn)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)p;
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
+
+// Device address of the static partials in the current context of device
+// dev.  Resolved once per context: a cudaDeviceReset (or any new context on
+// the same ordinal) changes the context id and the address is looked up
+// again, so a stale address from a destroyed context is never used.
 static double* static_dot_parts(int dev)
 {
     constexpr int kMaxDevices = 64;
+    struct Entry { unsigned long long ctx; double* addr; };
     static std::mutex mu;
-    static double* addr[kMaxDevices] = {};
+    static Entry cache[kMaxDevices] = {};
     if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    Entry& e = cache[dev];
+    if (!e.addr || ctx == 0 || e.ctx != ctx) {
         void* p = nullptr;
-        // The current device is dev, so the symbol resolves in its context.
+        // The current device is dev, so the symbol resolves in its context
+        // (the runtime makes the primary context current here if no call
+        // has yet); the id is read again once that context exists.
         if (cudaGetSymbolAddress(&p, gm::g_static_dot_parts) != cudaSuccess) return nullptr;
-        addr[dev] = static_cast<double*>(p);
+        e.addr = static_cast<double*>(p);
+        e.ctx = current_context_id();
     }
-    return addr[dev];
+    return e.addr;
 }
 
 extern "C" int gm_inner_prod_f64_noalloc(double* result, const float* x, const float* y, int len, void* stream)

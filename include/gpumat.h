@@ -30,6 +30,14 @@
 #include <stddef.h>
 #include <stdint.h>
 
+/* Default arguments of the reference's C++ declarations (Vector.cu:23,37,43),
+ * present when the header is compiled as C++ and absent in C. */
+#ifdef __cplusplus
+#define GM_DEFAULT(v) = v
+#else
+#define GM_DEFAULT(v)
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -76,11 +84,12 @@ void bmCopyToDevice(BandedMatrix* dA, const BandedMatrix* hA);
 void bmDeviceFree(BandedMatrix* dA);
 /* Vector.cu:23-30: zeroed device vector of length+lpad+rpad floats; *dx
  * points at element 0 (after the left pad). */
-void vecDeviceMalloc(float** dx, int length, int leftPadding, int rightPadding);
+void vecDeviceMalloc(float** dx, int length, int leftPadding GM_DEFAULT(0), int rightPadding GM_DEFAULT(0));
 /* Vector.cu:37-41 */
-void vecCopyToDevice(float** dx, const float* hx, int length, int leftPadding, int rightPadding);
+void vecCopyToDevice(float** dx, const float* hx, int length, int leftPadding GM_DEFAULT(0),
+                     int rightPadding GM_DEFAULT(0));
 /* Vector.cu:43-46 */
-void vecDeviceFree(float* dx, int leftPadding);
+void vecDeviceFree(float* dx, int leftPadding GM_DEFAULT(0));
 
 /* main.cu:57 / :458-526: `iterations` CG iterations on L alpha = b (device
  * data, alpha padded by `pad`), restarting every restartInterval. */
@@ -92,18 +101,33 @@ void jacobi(float* x, const BandedMatrix a, const float* b, float omega, int pad
 
 /* Matting.cu:39-219: Levin Laplacian + scribbles into the 25-band store.
  * HOST pointers, as in the reference; the work runs on the GPU with the
- * reference's arithmetic (results bit-identical) and gamma = 1. */
+ * reference's arithmetic (results bit-identical) and gamma = 1.  Unlike the
+ * reference's CPU loop it needs a CUDA device: it allocates device buffers
+ * and copies synchronously on each call, and without a usable device it
+ * sets GM_ERR_NOMEM or GM_ERR_CUDA and leaves L.a and b untouched. */
 void hostLevinLaplacian(BandedMatrix L, float* b, float lambda, gm_float4* im,
                         unsigned char* scribs, int imW, int imH, size_t imPitch);
 
-/* Solve.cpp:3-33 / Solve.h:17.  HOST vectors.  Runs on the GPU as a
- * multi-colour (9 colours over the 5x5 stencil) Gauss-Seidel sweep: same
- * fixed point as the sequential sweep, different visiting order. */
+/* Solve.cpp:3-33 / Solve.h:17.  HOST matrix and vectors, any band pattern
+ * (middle band = diagonal, as in the reference); x must be addressable
+ * max |offset| elements either side, as the reference reads it.  Runs on the
+ * GPU over a level schedule of the sequential sweep (rows whose non-zero
+ * couplings to earlier rows are all to earlier levels update together), so
+ * every iterate is bit-identical to the reference's sequential sweep for
+ * finite data.  Needs a CUDA device; the arithmetic never runs on the host. */
 void gaussSeidel_host(float* x, const BandedMatrix* A, const float* b, size_t iterations);
-/* Solve.cpp:35-85 / Solve.h:31.  HOST vectors (x padded by xpad); runs the
- * damped Jacobi iteration on the GPU and returns the last iterate in x. */
+/* Solve.cpp:35-85 / Solve.h:31.  HOST matrix and vectors (x padded by xpad
+ * >= max |offset|); the damped Jacobi iteration with the reference's FP32
+ * operation order on the GPU, bit-identical iterates.  The last iterate
+ * always ends in x (the reference loses it when `iterations` is odd,
+ * Solve.cpp:72-83). */
 void jacobi_host(float* x, const BandedMatrix* A, const float* b, size_t iterations, int xpad,
                  float omega);
+/* Levels of gaussSeidel_host's schedule for a host matrix: the number of
+ * dependent steps of one sweep (W + 3H - 3 or fewer for the Levin stencil
+ * of a W x H image; `rows` for a pattern whose rows form one chain).  -1 on
+ * bad arguments.  No counterpart in the reference. */
+int gm_gs_host_levels(const BandedMatrix* A);
 
 /* main.cu:558-577: prints "Ground truth MSE: %.3e" for HOST alpha/gt. */
 void computeError(float* alpha, float* gtAlpha, int imW, int imH);
@@ -137,7 +161,10 @@ int gm_inner_prod_f64(double* result, const float* x, const float* y, int len, v
  * more than 4096 partials are rejected (GM_ERR_INVALID; never on a 148-SM
  * B200, which uses at most 592); calls that overlap in time on one device
  * share the array and race, so serialise them; make the first call on each
- * device outside stream capture, since it resolves the array's address. */
+ * device outside stream capture, since it resolves the array's address.  The
+ * address is resolved again whenever the device's context changes (after a
+ * cudaDeviceReset, say), so the first call after such a change must also
+ * come outside stream capture. */
 int gm_inner_prod_f64_noalloc(double* result, const float* x, const float* y, int len, void* stream);
 /* Vector.cu:124-183 */
 int gm_vec_add(float* result, const float* x, const float* y, int len, void* stream);
@@ -417,5 +444,28 @@ int gm_banded_solve(BandedMatrix L, int W, float* alpha, int pad, const float* b
 
 #ifdef __cplusplus
 }
+
+/* Solve.h:17 and :31 take the matrix by const reference and default
+ * `iterations` and `omega`; these overloads let the reference's C++ callers
+ * (main.cu:264, :267) compile unchanged against this header.  They forward
+ * to the C entry points above. */
+inline void gaussSeidel_host(float* x, const BandedMatrix& A, const float* b, size_t iterations = 1)
+{
+    gaussSeidel_host(x, &A, b, iterations);
+}
+inline void jacobi_host(float* x, const BandedMatrix& A, const float* b, size_t iterations, int xpad,
+                        float omega = 2.f / 3.f)
+{
+    jacobi_host(x, &A, b, iterations, xpad, omega);
+}
+#if defined(__VECTOR_TYPES_H__)
+/* Matting.cu:39 takes CUDA's float4 (same layout as gm_float4); available
+ * when the caller has included the CUDA runtime headers first. */
+inline void hostLevinLaplacian(BandedMatrix L, float* b, float lambda, float4* im, unsigned char* scribs, int imW,
+                               int imH, size_t imPitch)
+{
+    hostLevinLaplacian(L, b, lambda, reinterpret_cast<gm_float4*>(im), scribs, imW, imH, imPitch);
+}
+#endif
 #endif
 #endif /* GPUMAT_H */

@@ -15,7 +15,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBORC = os.path.join(HERE, "liborc.so")
 LIBREF = os.path.join(HERE, "_ref", "libgmref.so")
-REF_TREE = "/root/reference"
+# The reference tree (rocketman768/gpumatting sources), used only to build
+# oracle/_ref: GM_REFERENCE_TREE when set, else a "reference" directory beside
+# the repository.
+REF_TREE = os.environ.get("GM_REFERENCE_TREE") or os.path.abspath(os.path.join(HERE, "..", "..", "reference"))
 
 _d = C.POINTER(C.c_double)
 _f = C.POINTER(C.c_float)

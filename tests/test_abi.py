@@ -59,3 +59,25 @@ def test_struct_layout_matches_reference():
     assert ctypes.sizeof(BandedMatrix) == 40
     assert BandedMatrix.apitch.offset == 8 and BandedMatrix.bands.offset == 16
     assert BandedMatrix.nbands.offset == 24 and BandedMatrix.rows.offset == 28 and BandedMatrix.cols.offset == 32
+
+
+def test_noalloc_dot_refuses_bad_operands_before_the_call():
+    """The Python wrapper checks dtype, device and length before handing
+    pointers to the library: the entry point writes one FP64 value into out
+    and reads len floats from x and y, so a float32 or host out, or a short
+    y, would be an out-of-bounds access on the device."""
+    import pytest
+    import torch
+
+    from gpumatting_b200 import api
+
+    x = torch.zeros(8)
+    out = torch.zeros(1, dtype=torch.float64)
+    with pytest.raises(ValueError):  # host tensors
+        api.inner_prod_noalloc(x, x, out)
+    with pytest.raises(TypeError):
+        api.inner_prod_noalloc(x.double(), x.double(), out)
+    with pytest.raises((TypeError, ValueError)):
+        api.inner_prod_noalloc(x, x, None)
+    with pytest.raises((TypeError, ValueError)):
+        api.inner_prod_noalloc(x, torch.zeros(4), out)

@@ -1,5 +1,6 @@
 """The C-ABI from C, compiled with gcc against include/gpumat.h and the
-in-tree libgpumat.so (the header is plain C) and run on the GPU.
+in-tree libgpumat.so (the header is plain C) and run on the GPU, and from
+C++ with the reference's own call forms (tests/c/test_cxx_callers.cpp).
 
 tests/c/test_dropin.c follows the reference's main.cu call sequence
 (hostLevinLaplacian, bmCopyToDevice, vecCopyToDevice, cgSolve / gradSolve,
@@ -15,18 +16,26 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-PROGRAMS = ("test_dropin", "test_native")
+PROGRAMS = ("test_dropin", "test_native", "test_cxx_callers")
 
 
 def _build(name: str, out: str) -> None:
-    if shutil.which("gcc") is None:
-        pytest.skip("gcc not available")
+    cxx = os.path.exists(os.path.join(ROOT, "tests", "c", name + ".cpp"))
+    compiler = "g++" if cxx else "gcc"
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not available")
     lib = os.path.join(ROOT, "gpumatting_b200")
-    cmd = ["gcc", "-std=c99", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
-           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "c", name + ".c"),
+    # C++: the reference's call forms (by-reference matrices, defaulted
+    # arguments, float4 images); FMA contraction off so the program's own
+    # host loops round as the reference's host build does
+    std = ["-std=c++17", "-ffp-contract=off"] if cxx else ["-std=c99"]
+    src = os.path.join(ROOT, "tests", "c", name + (".cpp" if cxx else ".c"))
+    cmd = [compiler, *std, "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(CUDA, "include"), src,
            "-L", lib, "-lgpumat", "-L", os.path.join(CUDA, "lib64"), "-lcudart",
            f"-Wl,-rpath,{lib}", f"-Wl,-rpath,{os.path.join(CUDA, 'lib64')}", "-lm", "-o", out]
-    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
 
 
 @pytest.mark.parametrize("name", PROGRAMS)
@@ -46,6 +55,13 @@ def _run(tmp_path, name: str) -> str:
 @pytest.mark.gpu
 def test_c_program_runs_the_reference_sequence(tmp_path):
     assert "Ground truth MSE" in _run(tmp_path, "test_dropin")
+
+
+@pytest.mark.gpu
+def test_cxx_program_makes_the_reference_calls(tmp_path):
+    """main.cu's C++ call forms compile unchanged against gpumat.h and give
+    the reference's arithmetic (see tests/c/test_cxx_callers.cpp)."""
+    assert "cg rel-res" in _run(tmp_path, "test_cxx_callers")
 
 
 @pytest.mark.gpu

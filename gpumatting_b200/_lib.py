@@ -64,7 +64,8 @@ class GmSolveParams(C.Structure):
 
 class GmSolveInfo(C.Structure):
     _fields_ = [("status", C.c_int), ("iters", C.c_int), ("replacements", C.c_int), ("rel_residual", C.c_double),
-                ("bnorm", C.c_double), ("kernel_ms", C.c_float), ("grid", C.c_int), ("where", C.c_int)]
+                ("bnorm", C.c_double), ("kernel_ms", C.c_float), ("grid", C.c_int), ("where", C.c_int),
+                ("solver", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -284,9 +284,12 @@ class SolveResult:
     kernel_ms: float
     grid: int
 
+    solver: str = ""
+
     @classmethod
     def from_info(cls, info: L.GmSolveInfo) -> "SolveResult":
-        return cls(info.status, info.iters, info.replacements, info.rel_residual, info.kernel_ms, info.grid)
+        name = {v: k for k, v in SOLVERS.items()}.get(info.solver, str(info.solver))
+        return cls(info.status, info.iters, info.replacements, info.rel_residual, info.kernel_ms, info.grid, name)
 
 
 class LevinStore:
@@ -398,8 +401,13 @@ class LevinStore:
             L.check(rc)
         return SolveResult.from_info(info)
 
-    def adjoint(self, alpha, dalpha, solver: str = "cg", want_dgamma: bool = True, stream=None, **params):
+    def adjoint(self, alpha, dalpha, solver: str = "mg", want_dgamma: bool = True, stream=None, **params):
         """Gradients of a loss of alpha through solve and assembly.
+
+        The lambda solve defaults to the multigrid-preconditioned CG, the one
+        solver that converges on this right-hand side at every size and eps
+        tried (CG and Jacobi PCG stall at 4096^2 with eps = 1e-7; asked for,
+        they fall back to it when they do not converge).
 
         dalpha = dloss/dalpha ([H, W] device floats).  Returns (dimage, dgamma,
         lam, SolveResult of the lam solve): dimage has the channel count of the

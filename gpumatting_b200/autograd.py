@@ -2,8 +2,8 @@
 
 alpha = levin_matte(image, gamma, s) assembles the Levin Laplacian of the
 [0, 1] RGB image (Matting.cu:79-218 math, eps as a parameter), solves
-(L + diag(gamma)) alpha = gamma * s on the GPU with the fused mixed-precision
-CG, and on backward runs gm_levin_adjoint: one more solve of the symmetric
+(L + diag(gamma)) alpha = gamma * s on the GPU (multigrid-preconditioned CG
+by default), and on backward runs gm_levin_adjoint: one more solve of the symmetric
 system for lambda, then the window-statistics back-propagation to the image
 and lambda * (s - alpha) for gamma.  The reference has no gradients; this is
 the differentiable form of its cgSolve path (main.cu:458-526).
@@ -49,10 +49,12 @@ class LevinMatte(torch.autograd.Function):
 
 
 def levin_matte(image, gamma, s, eps: float = 1e-5, precision: str = "fp16", rtol: float = 1e-6,
-                max_iters: int = 5000, adjoint_rtol: float | None = None, solver: str = "cg"):
+                max_iters: int = 5000, adjoint_rtol: float | None = None, solver: str = "mg"):
     """Differentiable matte: alpha (H, W) from image (H, W, 3) in [0, 1],
     per-pixel scribble weights gamma and targets s (both (H, W)).  solver:
-    "cg", "pcg" (Jacobi-preconditioned) or "mg" (multigrid-preconditioned)
-    for both the solve and the adjoint."""
+    "mg" (multigrid-preconditioned CG, the default: the fastest solve, and the
+    one whose adjoint converges at every size and eps tried), "cg" or "pcg"
+    (Jacobi-preconditioned) for both the solve and the adjoint; an adjoint
+    solve with "cg" or "pcg" that does not converge is redone with "mg"."""
     return LevinMatte.apply(image, gamma, s, eps, precision, rtol, max_iters,
                             rtol if adjoint_rtol is None else adjoint_rtol, solver)

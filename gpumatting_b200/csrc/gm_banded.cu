@@ -249,6 +249,7 @@ int generic_solve(const BandedMatrix& L, float* alpha, int pad, const float* b, 
         info->bnorm = std::sqrt(bb_host);
         info->rel_residual = std::sqrt(rr_true / (bb_host > 0 ? bb_host : 1.0));
         info->status = rc;
+        info->solver = p.solver;
         if (rc == GM_OK && p.rtol > 0 && !(info->rel_residual <= p.rtol)) info->status = GM_ERR_NOT_CONVERGED;
     }
     return rc == GM_OK && info ? info->status : rc;

@@ -176,8 +176,25 @@ extern "C" int gm_levin_adjoint(const gm_levin_store* store, const gm_image* im,
     }
     const int W = store->W, H = store->H;
     cudaStream_t st = (cudaStream_t)stream;
+    gm_solve_params p;
+    if (prm) p = *prm; else gm_default_params(&p);
+    gm_solve_info first;
+    gm_solve_info* inf = info ? info : &first;
     GM_CUDA_TRY(cudaMemsetAsync(lambda, 0, sizeof(float) * (size_t)W * H, st));
-    const int rc = levin_solve_impl(store, dalpha, W, lambda, prm, info, stream);
+    int rc = levin_solve_impl(store, dalpha, W, lambda, &p, inf, stream);
+    if (rc == GM_ERR_NOT_CONVERGED && p.solver != GM_SOLVER_MG) {
+        // The right-hand side dloss/dalpha excites the smooth, weakly
+        // constrained modes that a scribble-driven forward solve barely
+        // touches; at small eps or large sizes CG and Jacobi PCG stall on
+        // them.  Solve again with the multigrid-preconditioned CG from zero;
+        // info->solver says so, kernel_ms counts both solves.
+        const float ms0 = inf->kernel_ms;
+        gm_solve_params q = p;
+        q.solver = GM_SOLVER_MG;
+        GM_CUDA_TRY(cudaMemsetAsync(lambda, 0, sizeof(float) * (size_t)W * H, st));
+        rc = levin_solve_impl(store, dalpha, W, lambda, &q, inf, stream);
+        inf->kernel_ms += ms0;
+    }
     if (rc != GM_OK && rc != GM_ERR_NOT_CONVERGED) return rc;
     GM_TRY(gm_levin_adjoint_grads(im, sc, eps, W, H, lambda, alpha, dimage, dimage_pitch, dimage_channels, dgamma,
                                   st));

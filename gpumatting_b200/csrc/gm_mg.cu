@@ -1698,6 +1698,7 @@ int run_mg_solver(const gm_levin_store* store, const float* b, int bpitch, const
         info->kernel_ms = ms;
         info->grid = pl.L + 1;
         info->where = 0;
+        info->solver = GM_SOLVER_MG;
     }
     if (s.status != GM_OK) {
         gm_set_error_msg(s.status == GM_ERR_NOT_CONVERGED ? "multigrid CG: max_iters reached above rtol"
@@ -1718,6 +1719,7 @@ static void fill_info(gm_solve_info* info, const mg::State& s, float ms, int lev
     info->kernel_ms = ms;
     info->grid = levels;
     info->where = 0;
+    info->solver = GM_SOLVER_MG;
 }
 
 }  // namespace gm

@@ -302,6 +302,9 @@ typedef struct gm_solve_info_s {
     float kernel_ms;      /* device time of the solver kernel              */
     int grid;             /* CTAs launched                                  */
     int where;            /* which bounded wait gave up, if any            */
+    int solver;           /* GM_SOLVER_* that produced the result: the one
+                             asked for, or GM_SOLVER_MG after gm_levin_adjoint
+                             fell back to it                               */
 } gm_solve_info;
 
 void gm_default_params(gm_solve_params* p);
@@ -336,8 +339,12 @@ int gm_levin_solve_rhs(const gm_levin_store* st, const float* rhs, float* x, con
  *           pixel, rows dimage_pitch floats apart;
  *   dgamma: dloss/dgamma_i = lambda_i (s_i - alpha_i), [H][W], may be NULL
  *           (s_i is the scribble target, 0 on pixels without one).
- * im, sc and eps must be the ones the store was assembled with.  Returns the
- * lambda solve's status (GM_ERR_NOT_CONVERGED still writes the gradients). */
+ * im, sc and eps must be the ones the store was assembled with.  When the
+ * lambda solve with CG, Jacobi PCG, GD or Jacobi ends GM_ERR_NOT_CONVERGED
+ * (CG stalls on this right-hand side at small eps and large sizes), lambda is
+ * solved again from zero with GM_SOLVER_MG and info->solver says so.  Returns
+ * the final lambda solve's status (GM_ERR_NOT_CONVERGED still writes the
+ * gradients). */
 int gm_levin_adjoint(const gm_levin_store* st, const gm_image* im, const gm_scribbles* sc, double eps,
                      const float* alpha, const float* dalpha, float* lambda, float* dimage,
                      size_t dimage_pitch, int dimage_channels, float* dgamma, const gm_solve_params* p,

@@ -103,3 +103,62 @@ def test_autograd_512_matches_finite_differences(solver):
         # per pixel: 1e-3 relative, with a floor at 1e-3 of the largest sample
         floor = 1e-3 * np.abs(fd).max()
         assert np.all(np.abs(got - fd) <= 1e-3 * np.abs(fd) + floor)
+
+
+def test_default_adjoint_converges_at_1024_eps1e7(orc):
+    """The large-configuration adjoint on the default path: at eps = 1e-7 the
+    lambda solve of CG and Jacobi PCG stalls (4096^2), so the adjoint's
+    default solver is the multigrid PCG.  Checked here: it converges; lambda
+    has a true FP64 relative residual of 1e-6 (host, oracle operator over
+    the store's FP32 planes); the image gradient equals the FP64 window
+    back-propagation (oracle.levin_backward64) of the GPU's own lambda and
+    alpha within 1e-3; dgamma = lambda (s - alpha)."""
+    torch = torch_cuda()
+    W = H = 1024
+    p = make_problem(W, H, 0, eps=1e-7)
+    im, gamma, s, gt = _inputs(torch, p)
+    im4 = torch.zeros((H, W, 4), device="cuda")
+    im4[..., :3] = im
+    st = api.LevinStore(W, H, "fp16").assemble(im4, gamma_map=gamma, s_map=s, eps=p.eps)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    r = st.solve(alpha, rtol=1e-6, max_iters=5000)
+    assert r.status == 0, r
+    dalpha = 2.0 * (alpha - gt) / (W * H)
+    dimage, dgamma, lam, ra = st.adjoint(alpha, dalpha, rtol=1e-6, max_iters=5000)
+    print(f"1024^2 eps 1e-7 default adjoint: {ra}")
+    assert ra.status == 0 and ra.solver == "mg" and ra.rel_residual <= 1e-6, ra
+    g = p.gamma.ravel().astype(np.float64)
+    w32 = st.planes("w32")[:, :, :W].reshape(12, -1).double().cpu().numpy()
+    op = orc.Operator(W=W, H=H, w=w32, gamma=g)
+    rhs = dalpha.double().cpu().numpy().ravel()
+    lam64 = lam.double().cpu().numpy().ravel()
+    assert np.linalg.norm(rhs - op.apply(lam64)) / np.linalg.norm(rhs) <= 1.05e-6
+    a64 = alpha.double().cpu().numpy().ravel()
+    im3 = im.double().cpu().numpy()
+    want = orc.levin_backward64(orc.sym_edge_grad(lam64, a64, W, H), im3, p.eps)
+    assert _rel(dimage[..., :3].cpu().numpy(), want) <= 1e-3
+    assert _rel(dgamma.cpu().numpy().ravel(), lam64 * (p.s.ravel() - a64)) <= 1e-5
+
+
+def test_adjoint_falls_back_to_multigrid(orc):
+    """A CG lambda solve that ends above rtol is redone from zero with the
+    multigrid PCG: the result says so and equals the multigrid adjoint bit
+    for bit."""
+    torch = torch_cuda()
+    W, H = 96, 64
+    p = make_problem(W, H, 2)
+    im, gamma, s, gt = _inputs(torch, p)
+    im4 = torch.zeros((H, W, 4), device="cuda")
+    im4[..., :3] = im
+    st = api.LevinStore(W, H, "fp16").assemble(im4, gamma_map=gamma, s_map=s, eps=p.eps)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    st.solve(alpha, "mg", rtol=1e-9, max_iters=2000)
+    dalpha = 2.0 * (alpha - gt) / (W * H)
+    d1, g1, l1, r1 = st.adjoint(alpha, dalpha, "cg", rtol=1e-9, max_iters=400)  # CG needs more
+    d2, g2, l2, r2 = st.adjoint(alpha, dalpha, "mg", rtol=1e-9, max_iters=400)
+    assert r1.solver == "mg" and r2.solver == "mg" and r1.status == 0, (r1, r2)
+    assert r1.iters == r2.iters
+    for a, b in ((d1, d2), (g1, g2), (l1, l2)):
+        assert torch.equal(a, b)
+    d3, _, _, r3 = st.adjoint(alpha, dalpha, "cg", rtol=1e-9, max_iters=20000)  # converges: no fallback
+    assert r3.solver == "cg" and r3.status == 0, r3

@@ -250,14 +250,44 @@ def run_reference(args):
     value = threads * N * sweeps * args.steps / 1e6 / total
     sample = (f"{args.W}x{args.H} image per thread: hostLevinLaplacian ({asm:.2f} s) + {sweeps} gaussSeidel_host "
               f"sweeps, {threads} independent images on {threads} threads")
+    conv = reference_convergence(prob, sweeps)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_dict(args),
+            "data": "synthetic", "config": reference_config_dict(args, sweeps, threads),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "iterations are Gauss-Seidel sweeps (Solve.cpp:3-33); the reference has no CPU CG"}
+            "time_to_rtol": conv,
+            "note": "units differ from the GPU arm: iterations here are Gauss-Seidel sweeps (Solve.cpp:3-33), "
+                    "the reference has no CPU CG; time_to_rtol gives the residual the sweeps reach"}
     print(json.dumps(line), flush=True)
+
+
+def reference_convergence(prob, sweeps: int) -> dict:
+    """How far the reference's CPU path gets towards rel-residual 1e-6: the
+    true FP64 relative residual ||b - A x|| / ||b|| of its own 25-band system
+    after `sweeps` gaussSeidel_host sweeps from alpha = 0.5 (one image, one
+    core), with the time those sweeps took.  Gauss-Seidel on this
+    ill-conditioned system does not reach 1e-6 in any affordable sample."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    W, H = prob.W, prob.H
+    im4 = prob.image_float4()
+    use_ref = O.ref_available()
+    a, b = O.ref_levin(im4, prob.scribbles, prob.eps) if use_ref else O.levin_ref32(im4, prob.scribbles, prob.eps, 1.0)
+    offs = O.levin_offsets(W)
+    op = O.Operator(W=W, H=H, bands=a.astype(np.float64), offs=offs)
+    b64 = b.astype(np.float64)
+    x = np.full(W * H, 0.5, np.float32)
+    rel0 = float(np.linalg.norm(b64 - op.apply(x.astype(np.float64))) / np.linalg.norm(b64))
+    t0 = time.perf_counter()
+    x = O.gs_host(a, offs, b, x, sweeps, use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    rel = float(np.linalg.norm(b64 - op.apply(x.astype(np.float64))) / np.linalg.norm(b64))
+    return {"target_rel_residual": 1e-6, "reached": rel <= 1e-6, "sweeps": sweeps, "seconds": dt,
+            "rel_residual_start": rel0, "rel_residual_reached": rel, "cores": 1}
 
 
 def config_dict(args) -> dict:
@@ -266,6 +296,17 @@ def config_dict(args) -> dict:
                         f"(FP64 replacement every 50, max 5000)",
             "W": args.W, "H": args.H, "precision": args.precision, "rtol": 1e-6,
             "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
+
+
+def reference_config_dict(args, sweeps: int, threads: int) -> dict:
+    """What the reference arm runs: the reference's CPU solve path on the same
+    synthetic image, a fixed number of Gauss-Seidel sweeps (it has no CPU CG
+    and no stopping rule), one independent image per host thread."""
+    return {"workload": f"{args.W}x{args.H} synthetic matting solve (seeded), eps=1e-5, gamma=1 (Matting.cu:48), "
+                        f"~10% scribbles; reference CPU path: hostLevinLaplacian into 25 FP32 bands, then "
+                        f"{sweeps} gaussSeidel_host sweeps (Solve.cpp:3-33), fixed count",
+            "W": args.W, "H": args.H, "precision": "fp32 (25 bands)", "sweeps": sweeps, "threads": threads,
+            "parallelism": f"{threads} independent images on {threads} host threads"}
 
 
 # ---------------------------------------------------------------------------
@@ -476,9 +517,25 @@ def run_ours(args):
         # to the same true rel-res (the plain arm's 25 bands are assembled once,
         # outside its timing); the *_step_* ratios put the mixed arm's assembly
         # on its side only (conservative)
-        pl = run_plain(args, prob, img_d, scr_d, flush, stream)
-        pl["speedup_mixed_vs_plain"] = pl["ms_per_solve"] / line["solve_only_ms"]
+        def mixed_once(i):
+            store.assemble(img_d, scr_d, eps=prob.eps, gamma_value=100.0)
+            alpha.copy_(a0_d, non_blocking=True)
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = store.solve(alpha, args.solver, **params)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1), r
+
+        pl = run_plain(args, prob, img_d, scr_d, flush, stream, mixed_once)
+        pl["speedup_mixed_vs_plain"] = pl["speedup_median"]
         pl["speedup_mixed_step_vs_plain_solve"] = pl["ms_per_solve"] / line["ms_per_step"]
+        # the north-star target numbers, where a reader of the line sees them first
+        line["speedup_mixed_vs_plain"] = pl["speedup_median"]
+        line["speedup_mixed_vs_plain_range"] = [pl["speedup_per_round_min"], pl["speedup_per_round_max"]]
+        line["plain_fp32_ms"] = pl["ms_per_solve"]
+        line["mixed_cg_solve_ms"] = pl["mixed_ms_per_solve"]
         if "pcg" in line:
             pl["speedup_mixed_pcg_vs_plain"] = pl["ms_per_solve"] / line["pcg"]["solve_only_ms"]
         if "mg" in line:
@@ -501,11 +558,25 @@ def run_ours(args):
                                 "sample": f"{W}x{H}: hostLevinLaplacian ({asm:.2f} s) + {sweeps} gaussSeidel_host "
                                           f"sweeps on 1 core (iterations are Gauss-Seidel sweeps)"}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(ordered_line(line)), flush=True)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# Keys printed first: the contract's, then the headline target numbers; the
+# supplementary sections follow in the order they ran.
+LEAD_KEYS = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+             "vs_baseline", "dtype", "data", "config", "time_to_rtol_ms", "speedup_mixed_vs_plain",
+             "speedup_mixed_vs_plain_range", "plain_fp32_ms", "mixed_cg_solve_ms", "time_to_rtol_mg_ms", "roofline",
+             "e2e", "gpu_launches", "clocks", "cpu_baseline")
+
+
+def ordered_line(line: dict) -> dict:
+    out = {k: line[k] for k in LEAD_KEYS if k in line}
+    out.update((k, v) for k, v in line.items() if k not in out)
+    return out
 
 
 # Multigrid PCG on an FP16 store, algorithmic bytes per pixel-iteration:
@@ -830,8 +901,11 @@ def run_solvers(args, prob, img_d, scr_d, store, flush, stream) -> dict:
     return out
 
 
-def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
-    """Plain FP32 method: 25-band FP32 store + fused CG to 1e-6."""
+def run_plain(args, prob, img_d, scr_d, flush, stream, mixed_once) -> dict:
+    """Plain FP32 method (25-band FP32 store + fused CG to 1e-6) timed
+    interleaved with the mixed arm: each round solves with both (order
+    alternating between rounds), L2 flushed before every solve, so clock or
+    thermal drift hits both arms alike.  mixed_once(i) -> (ms, result)."""
     import numpy as np
     import torch
 
@@ -842,8 +916,8 @@ def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
     a, b = api.levin_bands25(img_d, scr_d, eps=prob.eps, gamma_value=100.0, arithmetic="fp64")
     Lm = api.DeviceBandedMatrix(a, torch.tensor(api.levin_band_offsets(W), device=a.device), N)
     x = api.PaddedVector(N, api.levin_pad(W))
-    res_all, ms = [], []
-    for i in range(2 + args.plain_steps):
+
+    def plain_once(i):
         x.data.fill_(0.5)
         flush.fill_(float(i))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -851,16 +925,32 @@ def run_plain(args, prob, img_d, scr_d, flush, stream) -> dict:
         r = api.banded_solve(Lm, x, b, W=W, solver="cg", rtol=1e-6, max_iters=5000, replace_every=50)
         e1.record(stream)
         torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    rounds = max(5, args.plain_steps)
+    res_all, ms, mixed_ms, mixed_res = [], [], [], []
+    for i in range(2 + rounds):
+        order = (plain_once, mixed_once) if i % 2 == 0 else (mixed_once, plain_once)
+        out = {f: f(2 * i + k) for k, f in enumerate(order)}
         if i >= 2:
-            res_all.append(r)
-            ms.append(e0.elapsed_time(e1))
+            ms.append(out[plain_once][0])
+            res_all.append(out[plain_once][1])
+            mixed_ms.append(out[mixed_once][0])
+            mixed_res.append(out[mixed_once][1])
+    assert all(r.status == 0 and r.rel_residual <= 1e-6 for r in mixed_res), mixed_res
     it = statistics.mean(r.iters for r in res_all)
     kms = statistics.mean(r.kernel_ms for r in res_all)
     reps = statistics.mean(r.replacements for r in res_all)
     alg = N * (it * KRYLOV_BYTES["ref25"] + reps * REPLACE_BYTES["ref25"] + IMPORT_BYTES["ref25"])
-    return {"ms_per_solve": statistics.mean(ms), "iters": it, "rel_residual": res_all[-1].rel_residual,
-            "mpix_iter_s": N * it / 1e6 / (statistics.mean(ms) / 1000), "kernel_ms": kms,
-            "achieved_gbs": alg / (kms / 1000) / 1e9, "status": res_all[-1].status}
+    ratios = [p / m for p, m in zip(ms, mixed_ms)]
+    return {"ms_per_solve": statistics.median(ms), "ms_min": min(ms), "ms_max": max(ms), "rounds": rounds,
+            "iters": it, "rel_residual": res_all[-1].rel_residual,
+            "mpix_iter_s": N * it / 1e6 / (statistics.median(ms) / 1000), "kernel_ms": kms,
+            "achieved_gbs": alg / (kms / 1000) / 1e9, "status": res_all[-1].status,
+            "mixed_ms_per_solve": statistics.median(mixed_ms), "mixed_ms_min": min(mixed_ms),
+            "mixed_ms_max": max(mixed_ms), "mixed_iters": statistics.mean(r.iters for r in mixed_res),
+            "speedup_median": statistics.median(ms) / statistics.median(mixed_ms),
+            "speedup_per_round_min": min(ratios), "speedup_per_round_max": max(ratios)}
 
 
 def main():

@@ -336,7 +336,8 @@ def run_ours(args):
     alpha = torch.empty((H, W), dtype=torch.float32, device=dev)
     store = api.LevinStore(W, H, args.precision)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MB > L2
-    params = dict(rtol=1e-6, max_iters=5000, replace_every=args.replace_every, ctas_per_sm=args.ctas_per_sm)
+    params = dict(rtol=1e-6, max_iters=5000, replace_every=args.replace_every, ctas_per_sm=args.ctas_per_sm,
+                  strip_width=args.strip_width)
     if args.fixed_iters:
         params.update(rtol=0.0, max_iters=args.fixed_iters)
 
@@ -984,6 +985,7 @@ def main():
     ap.add_argument("--large-only", action="store_true", help="profiling: only the large solve + adjoint")
     ap.add_argument("--replace-every", type=int, default=50)
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="ring configuration: 0 auto, 3 shallow, 2 deep")
+    ap.add_argument("--strip-width", type=int, default=0, help="fused solver strip width: 0 auto, 192, 128")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

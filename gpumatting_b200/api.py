@@ -486,7 +486,11 @@ class LevinBatch:
     def info(self) -> dict:
         v = [C.c_int() for _ in range(5)]
         L.check(L.load().gm_batch_info(self.h, *[C.byref(x) for x in v]))
-        return dict(zip(["ctas_per_sm", "ring_cfg", "row_mult", "graph_launches", "grid"], [x.value for x in v]))
+        d = dict(zip(["ctas_per_sm", "ring_cfg", "row_mult", "graph_launches", "grid"], [x.value for x in v]))
+        # launch configurations of the fused solver: 0, 1 = 192-column strips
+        # (shallow / deep rings), 2 = 128-column strips
+        d["strip_width"] = {0: 192, 1: 192, 2: 128}.get(d["ring_cfg"], 0)
+        return d
 
     def solve(self, alphas, solver: str = "cg", stream=None, **params) -> list:
         n = len(self.sizes)

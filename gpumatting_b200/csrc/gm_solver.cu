@@ -4,7 +4,7 @@
 // Jacobi (the reference's cgSolve / gradSolve / jacobi, main.cu:406-556),
 // each run as ONE cooperative kernel with no host round trip per iteration.
 //
-// Work decomposition.  The image is cut into column strips of kStrip (192)
+// Work decomposition.  The image is cut into column strips of 64 * NCOL
 // pixels and each strip into row segments; one CTA owns one (strip,
 // segment) unit and sweeps down it row by row.  A CTA is one TMA producer
 // warp and kConsumers consumer warps:
@@ -99,12 +99,12 @@ __device__ __forceinline__ const T* plane(const unsigned char* slot, int k, int 
 // X[d][m]: operand at row vbase + d - 2, local column 2*lane + m (output
 // pixel e sits at m = 2 + e); the output row is vbase + RO, so rows
 // RO..RO+4 of X are its stencil rows.  brow[d]: band slot of row v - d.
-template <class T, int K, int RO>
+template <class T, int K, int RO, int BOX>
 __device__ __forceinline__ void symd_term(float2& yu, float2& yl, const float (&X)[6][6],
                                           const unsigned char* const (&brow)[3], int c)
 {
     constexpr int du = sym_du(K), dv = sym_dv(K);
-    constexpr int pstride = kBox * (int)sizeof(T);
+    constexpr int pstride = BOX * (int)sizeof(T);
     const float2 wu = ld2(plane<T>(brow[0], K - 1, pstride), c);
     yu.x = fmaf(-wu.x, X[RO + 2 + dv][2 + du], yu.x);
     yu.y = fmaf(-wu.y, X[RO + 2 + dv][3 + du], yu.y);
@@ -115,36 +115,36 @@ __device__ __forceinline__ void symd_term(float2& yu, float2& yl, const float (&
 
 // Four independent accumulation chains per pixel (upper/lower x two halves
 // of the bands) keep the FMA dependency chains short.
-template <class T, int RO>
+template <class T, int RO, int BOX>
 __device__ __forceinline__ float2 symd_apply(const float (&X)[6][6], const unsigned char* const (&brow)[3], int xoff,
                                              int c)
 {
     const float2 dg = ld2(reinterpret_cast<const float*>(brow[0] + xoff), c);
     float2 a = make_float2(dg.x * X[RO + 2][2], dg.y * X[RO + 2][3]);
     float2 b = make_float2(0.f, 0.f), e = make_float2(0.f, 0.f), f = make_float2(0.f, 0.f);
-    symd_term<T, 1, RO>(a, b, X, brow, c);
-    symd_term<T, 2, RO>(e, f, X, brow, c);
-    symd_term<T, 3, RO>(a, b, X, brow, c);
-    symd_term<T, 4, RO>(e, f, X, brow, c);
-    symd_term<T, 5, RO>(a, b, X, brow, c);
-    symd_term<T, 6, RO>(e, f, X, brow, c);
-    symd_term<T, 7, RO>(a, b, X, brow, c);
-    symd_term<T, 8, RO>(e, f, X, brow, c);
-    symd_term<T, 9, RO>(a, b, X, brow, c);
-    symd_term<T, 10, RO>(e, f, X, brow, c);
-    symd_term<T, 11, RO>(a, b, X, brow, c);
-    symd_term<T, 12, RO>(e, f, X, brow, c);
+    symd_term<T, 1, RO, BOX>(a, b, X, brow, c);
+    symd_term<T, 2, RO, BOX>(e, f, X, brow, c);
+    symd_term<T, 3, RO, BOX>(a, b, X, brow, c);
+    symd_term<T, 4, RO, BOX>(e, f, X, brow, c);
+    symd_term<T, 5, RO, BOX>(a, b, X, brow, c);
+    symd_term<T, 6, RO, BOX>(e, f, X, brow, c);
+    symd_term<T, 7, RO, BOX>(a, b, X, brow, c);
+    symd_term<T, 8, RO, BOX>(e, f, X, brow, c);
+    symd_term<T, 9, RO, BOX>(a, b, X, brow, c);
+    symd_term<T, 10, RO, BOX>(e, f, X, brow, c);
+    symd_term<T, 11, RO, BOX>(a, b, X, brow, c);
+    symd_term<T, 12, RO, BOX>(e, f, X, brow, c);
     return make_float2((a.x + b.x) + (e.x + f.x), (a.y + b.y) + (e.y + f.y));
 }
 
 // True operator, implicit diagonal, accumulation type V (float or double);
 // also returns the diagonal gamma + sum w (for Jacobi).
-template <class V, int K, int RO>
+template <class V, int K, int RO, int BOX>
 __device__ __forceinline__ void symi_term(V& y0, V& y1, V& d0, V& d1, const V (&X)[6][6],
                                           const unsigned char* const (&brow)[3], int c)
 {
     constexpr int du = sym_du(K), dv = sym_dv(K);
-    constexpr int pstride = kBox * 4;
+    constexpr int pstride = BOX * 4;
     const float2 wu = ld2(plane<float>(brow[0], K - 1, pstride), c);
     const float2 wl = ld2s<du>(plane<float>(brow[dv], K - 1, pstride), c - du);
     y0 += (V)wu.x * (X[RO + 2][2] - X[RO + 2 + dv][2 + du]) + (V)wl.x * (X[RO + 2][2] - X[RO + 2 - dv][2 - du]);
@@ -153,7 +153,7 @@ __device__ __forceinline__ void symi_term(V& y0, V& y1, V& d0, V& d1, const V (&
     d1 += (V)wu.y + (V)wl.y;
 }
 
-template <class V, int RO>
+template <class V, int RO, int BOX>
 __device__ __forceinline__ void symi_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[6][6],
                                            const unsigned char* const (&brow)[3], int xoff, int c)
 {
@@ -162,27 +162,27 @@ __device__ __forceinline__ void symi_apply(V& y0, V& y1, V& d0, V& d1, const V (
     y1 = (V)g.y * X[RO + 2][3];
     d0 = (V)g.x;
     d1 = (V)g.y;
-    symi_term<V, 1, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 2, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 3, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 4, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 5, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 6, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 7, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 8, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 9, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 10, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 11, RO>(y0, y1, d0, d1, X, brow, c);
-    symi_term<V, 12, RO>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 1, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 2, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 3, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 4, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 5, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 6, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 7, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 8, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 9, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 10, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 11, RO, BOX>(y0, y1, d0, d1, X, brow, c);
+    symi_term<V, 12, RO, BOX>(y0, y1, d0, d1, X, brow, c);
 }
 
 // Reference layout: y = sum_j a_j x(u+du_j, v+dv_j), band j = 12 + du + 5 dv,
 // in band order (BandedMatrix.cu:172-173); d = a_12.
-template <class V, int RO>
+template <class V, int RO, int BOX>
 __device__ __forceinline__ void ref25_apply(V& y0, V& y1, V& d0, V& d1, const V (&X)[6][6],
                                             const unsigned char* b0, int c)
 {
-    constexpr int pstride = kBox * 4;
+    constexpr int pstride = BOX * 4;
     V s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0};  // three chains per pixel
 #pragma unroll
     for (int j = 0; j < 25; ++j) {
@@ -230,15 +230,19 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive_n(uint64_t* bar, uint32_t n)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(n) : "memory");
+}
 
 // Rows vbase-2 .. vbase+3 of the operand sit in ring rows r0, r0+1, ...
-// (mod 8); columns lc0 .. lc0+5.
-template <class V>
+// (mod NR); columns lc0 .. lc0+5.
+template <class V, int NR>
 __device__ __forceinline__ void load_rows(V (&X)[6][6], const V* ring, int r0, int lc0)
 {
 #pragma unroll
     for (int d = 0; d < 6; ++d) {
-        const V* row = ring + ((r0 + d) & 7) * kRingCols + lc0;
+        const V* row = ring + ((r0 + d) & (NR - 1)) * kRingCols + lc0;
 #pragma unroll
         for (int m = 0; m < 6; m += 2) {
             if constexpr (sizeof(V) == 4) {
@@ -260,6 +264,9 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
 {
     constexpr Layout L = make_layout(OPLO, OPLO == OP_REF25 ? 4 : (int)sizeof(TLo), OPHI, MIXED, CFG);
     constexpr KindLayout K = L.k[KIND];
+    constexpr int NCONS = cfg_ncol(CFG);
+    constexpr int BOX = cfg_box(CFG);
+    constexpr int OPR = kOpRows, OWNR = kOwnRows;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nsteps = v1 - v0 + 4;
     const int nband = nsteps - 2;
@@ -267,10 +274,10 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
     unsigned char* vring = smem + K.vbase;
     unsigned char* bring = smem + K.bbase;
-    volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + kRedBytes);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + cfg_red_bytes(CFG));
     constexpr bool kSymBand = (KIND == KIND_KRYLOV ? OPLO : OPHI) != OP_REF25;
 
-    if (warp == kConsumers) {
+    if (warp == NCONS) {
         // ------------------------------ producer ------------------------------
         if (lane != 0) return;
         const CUtensorMap* vm[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -348,32 +355,42 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     const int cx = lane == 0 ? 6 + kWarpCols * w : 8 + kWarpCols * w + kWarpCols;
     const int lcx = lane == 0 ? 0 : kRingCols - 2;
     using RingT = std::conditional_t<MIXED, double, float>;  // replacement operand ring element
-    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * 8 * kRingCols * (MIXED ? 2 : 1);
-    RingT* ring_d = reinterpret_cast<RingT*>(smem + L.pring_off) + w * 8 * kRingCols;
-    float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * 4 * kWarpCols;  // r or b, own columns
+    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * OPR * kRingCols * (MIXED ? 2 : 1);
+    RingT* ring_d = reinterpret_cast<RingT*>(smem + L.pring_off) + w * OPR * kRingCols;
+    float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * OWNR * kWarpCols;  // r or b, own columns
     const int P = A.P;
     constexpr int Rb = K.Rb;
     constexpr bool pcg = PCG && OPLO == OP_SYMD && KIND == KIND_KRYLOV;  // Jacobi-preconditioned CG
 
-    int vs = 0;    // vector slot of the next step
-    int bsn = 0;   // band slot of the next band step to wait for
-    int bwait = 0; // next band step to wait for
-    int brel = 0;  // next band step to release
-    int brel_s = 0;
+    int vs = 0;     // vector slot of the next vector row
+    int bs = 0;     // band slot of the next band step
+    // band steps j-4 .. j-1 of super-step j: slot (low byte) and full-barrier
+    // parity (bit 8), kept in registers as a sliding window
+    uint32_t bw0 = 0u, bw1 = 0u, bw2 = 0u, bw3 = 0u;
 
-    // phase A of step j into operand ring row (j & 7) and own ring row (j & 3)
-    auto phase_a = [&](int j) {
+    auto wait_rec = [&](uint32_t r) {
+        if (!*s_abort && !mbar_wait_bounded(&full[kRvMax + (r & 0xffu)], r >> 8, A.gb, A.tma_limit_ns))
+            *s_abort = 1;
+    };
+    auto band_of = [&](uint32_t r) { return bring + (int)(r & 0xffu) * K.bslot; };
+    // Band step m is read by the phase B of super-steps j (even, 4 <= j <
+    // nsteps) with j-4 <= m <= j-1 (symmetric store: output row v reads rows
+    // v, v-1, v-2) or m in {j-2, j-1} (reference layout: row v only).  Its
+    // slot is released at its last read, by all NCONS warps (the empty
+    // barrier takes 2 * NCONS arrivals, 2 per warp).
+    auto release_rec = [&](uint32_t r) {
+        if (lane == 0) mbar_arrive_n(&empty[kRvMax + (r & 0xffu)], 2u);
+    };
+
+    // phase A of step j (vector slot vsl, full parity vpar) into operand ring
+    // row j mod 8 and own ring row j mod 4
+    auto phase_a = [&](int j, int vsl, uint32_t vpar) {
         const int Lr = v0 - 2 + j;
-        {
-            const uint32_t bit = 1u << vs;
-            if (!*s_abort && !mbar_wait_bounded(&full[vs], (pp.full_v & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
-                *s_abort = 1;
-            pp.full_v ^= bit;
-        }
-        const unsigned char* vsp = vring + vs * K.vslot;
+        if (!*s_abort && !mbar_wait_bounded(&full[vsl], vpar, A.gb, A.tma_limit_ns)) *s_abort = 1;
+        const unsigned char* vsp = vring + vsl * K.vslot;
         const bool own_row = Lr >= v0 && Lr < v1;
         const size_t gi = (size_t)(own_row ? Lr : 0) * P + u;
-        const int rr = j & 7, orow = j & 3;
+        const int rr = j & (OPR - 1), orow = j & (OWNR - 1);
         if (KIND == KIND_KRYLOV) {
             const float* vr = reinterpret_cast<const float*>(vsp + K.voff[0]);
             const float* vq = reinterpret_cast<const float*>(vsp + K.voff[1]);
@@ -491,67 +508,85 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             if (own_row) *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = ld2(vb, c);
         }
     };
-    auto wait_band = [&]() {
-        const uint32_t bit = 1u << bsn;
-        if (!*s_abort && !mbar_wait_bounded(&full[kRvMax + bsn], (pp.full_b & bit) ? 1u : 0u, A.gb, A.tma_limit_ns))
-            *s_abort = 1;
-        pp.full_b ^= bit;
-        bsn = ring_next(bsn, Rb);
-        ++bwait;
-    };
-    auto release_bands_to = [&](int m_end) {  // release band steps [brel, m_end)
-        for (; brel < m_end; ++brel) {
-            if (lane == 0) mbar_arrive(&empty[kRvMax + brel_s]);
-            brel_s = ring_next(brel_s, Rb);
-        }
-    };
-    // band slot of band step m, given that bsn is the slot of step bwait
-    auto bslot_of = [&](int m) {
-        int sl = bsn - (bwait - m);
-        while (sl < 0) sl += Rb;
-        return sl;
-    };
-
     for (int j = 0; j < nsteps; j += 2) {
         const bool two = j + 1 < nsteps;
-        phase_a(j);
         const int vs0 = vs;
+        const uint32_t vp0 = (pp.full_v >> vs0) & 1u;
+        pp.full_v ^= 1u << vs0;
         vs = ring_next(vs, K.Rv);
+        int vs1 = 0;
+        uint32_t vp1 = 0u;
         if (two) {
-            phase_a(j + 1);
+            vs1 = vs;
+            vp1 = (pp.full_v >> vs1) & 1u;
+            pp.full_v ^= 1u << vs1;
             vs = ring_next(vs, K.Rv);
         }
+        // band steps j-2 and j-1 enter the window
+        bw0 = bw2;
+        bw1 = bw3;
+        if (j >= 2 && j - 2 < nband) {
+            bw2 = (uint32_t)bs | (((pp.full_b >> bs) & 1u) << 8);
+            pp.full_b ^= 1u << bs;
+            bs = ring_next(bs, Rb);
+        }
+        if (j >= 2 && j - 1 < nband) {
+            bw3 = (uint32_t)bs | (((pp.full_b >> bs) & 1u) << 8);
+            pp.full_b ^= 1u << bs;
+            bs = ring_next(bs, Rb);
+        }
+        phase_a(j, vs0, vp0);
+        if (two) phase_a(j + 1, vs1, vp1);
         __syncwarp();
         if (lane == 0) {
             mbar_arrive(&empty[vs0]);
-            if (two) mbar_arrive(&empty[ring_next(vs0, K.Rv)]);
+            if (two) mbar_arrive(&empty[vs1]);
         }
-        // band steps up to (last step of this super-step) - 2
-        const int mneed = (two ? j + 1 : j) - 2;
-        while (bwait <= mneed) wait_band();
+        if (!kSymBand && j == 2) {
+            // rows v0-2, v0-1: loaded but unused by the reference layout; released
+            // as soon as their loads land, since a ring of two slots needs them back
+            wait_rec(bw2);
+            wait_rec(bw3);
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_n(&empty[kRvMax + (bw2 & 0xffu)], 2u);
+                mbar_arrive_n(&empty[kRvMax + (bw3 & 0xffu)], 2u);
+            }
+        }
         if (j >= 4) {
             // ---------------- phase B: output rows v and v+1 ----------------
             const int v = v0 - 4 + j;
             const bool second = two && v + 1 < v1;
-            const unsigned char* bA[3] = {bring + bslot_of(j - 2) * K.bslot, bring + bslot_of(j - 3) * K.bslot,
-                                          bring + bslot_of(j - 4) * K.bslot};
-            const unsigned char* bB[3] = {bring + bslot_of(j - 1) * K.bslot, bA[0], bA[1]};
-            const int r0 = (j - 4) & 7;   // ring row of operand row v - 2
-            const int o0 = (j - 2) & 3;   // own ring row of output row v
-            const int o1 = (j - 1) & 3;
+            if (kSymBand) {
+                // steps j-4, j-3 were waited for at super-step j-2
+                if (j == 4) {
+                    wait_rec(bw0);
+                    wait_rec(bw1);
+                }
+                wait_rec(bw2);
+                if (second) wait_rec(bw3);
+            } else {
+                wait_rec(bw2);
+                if (second) wait_rec(bw3);
+            }
+            const unsigned char* bA[3] = {band_of(bw2), band_of(bw1), band_of(bw0)};
+            const unsigned char* bB[3] = {band_of(bw3), bA[0], bA[1]};
+            const int r0 = (j - 4) & (OPR - 1);   // ring row of operand row v - 2
+            const int o0 = (j - 2) & (OWNR - 1);  // own ring row of output row v
+            const int o1 = (j - 1) & (OWNR - 1);
             const size_t go = (size_t)v * P + u;
             if (in0) {
                 if (KIND == KIND_KRYLOV) {
                     float X[6][6];
-                    load_rows<float>(X, ring_f, r0, lc0);
+                    load_rows<float, OPR>(X, ring_f, r0, lc0);
                     float2 q0, q1 = make_float2(0.f, 0.f);
                     if (OPLO == OP_SYMD) {
-                        q0 = symd_apply<TLo, 0>(X, bA, K.xoff, c);
-                        if (second) q1 = symd_apply<TLo, 1>(X, bB, K.xoff, c);
+                        q0 = symd_apply<TLo, 0, BOX>(X, bA, K.xoff, c);
+                        if (second) q1 = symd_apply<TLo, 1, BOX>(X, bB, K.xoff, c);
                     } else {
                         float d0, d1;
-                        ref25_apply<float, 0>(q0.x, q0.y, d0, d1, X, bA[0], c);
-                        if (second) ref25_apply<float, 1>(q1.x, q1.y, d0, d1, X, bB[0], c);
+                        ref25_apply<float, 0, BOX>(q0.x, q0.y, d0, d1, X, bA[0], c);
+                        if (second) ref25_apply<float, 1, BOX>(q1.x, q1.y, d0, d1, X, bB[0], c);
                     }
                     // own ring: z (= r for plain CG) of the output rows
                     const float2 rn0 = *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0);
@@ -599,10 +634,10 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                 } else if (KIND == KIND_REPLACE) {
                     double X[6][6];
                     if constexpr (MIXED) {
-                        load_rows<double>(X, ring_d, r0, lc0);
+                        load_rows<double, OPR>(X, ring_d, r0, lc0);
                     } else {
                         float Xf[6][6];
-                        load_rows<float>(Xf, ring_d, r0, lc0);
+                        load_rows<float, OPR>(Xf, ring_d, r0, lc0);
 #pragma unroll
                         for (int a = 0; a < 6; ++a)
 #pragma unroll
@@ -623,18 +658,18 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         }
                     };
                     double y0, y1, d0, d1;
-                    if (OPHI == OP_REF25) ref25_apply<double, 0>(y0, y1, d0, d1, X, bA[0], c);
-                    else symi_apply<double, 0>(y0, y1, d0, d1, X, bA, K.xoff, c);
+                    if (OPHI == OP_REF25) ref25_apply<double, 0, BOX>(y0, y1, d0, d1, X, bA[0], c);
+                    else symi_apply<double, 0, BOX>(y0, y1, d0, d1, X, bA, K.xoff, c);
                     rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, v, 0);
                     if (second) {
-                        if (OPHI == OP_REF25) ref25_apply<double, 1>(y0, y1, d0, d1, X, bB[0], c);
-                        else symi_apply<double, 1>(y0, y1, d0, d1, X, bB, K.xoff, c);
+                        if (OPHI == OP_REF25) ref25_apply<double, 1, BOX>(y0, y1, d0, d1, X, bB[0], c);
+                        else symi_apply<double, 1, BOX>(y0, y1, d0, d1, X, bB, K.xoff, c);
                         rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0), go + P,
                                 v + 1, 1);
                     }
                 } else {  // Jacobi
                     float X[6][6];
-                    load_rows<float>(X, ring_f, r0, lc0);
+                    load_rows<float, OPR>(X, ring_f, r0, lc0);
                     auto jac_row = [&](float y0, float y1, float d0, float d1, const float2 bv, size_t g, int ro) {
                         const float rv0 = bv.x - y0, rv1 = bv.y - y1;
                         A.xacc[s.xsel ^ 1][g] = X[ro + 2][2] + A.omega * rv0 / d0;
@@ -647,27 +682,34 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         }
                     };
                     float y0, y1, d0, d1;
-                    if (OPHI == OP_REF25) ref25_apply<float, 0>(y0, y1, d0, d1, X, bA[0], c);
-                    else symi_apply<float, 0>(y0, y1, d0, d1, X, bA, K.xoff, c);
+                    if (OPHI == OP_REF25) ref25_apply<float, 0, BOX>(y0, y1, d0, d1, X, bA[0], c);
+                    else symi_apply<float, 0, BOX>(y0, y1, d0, d1, X, bA, K.xoff, c);
                     jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, 0);
                     if (second) {
-                        if (OPHI == OP_REF25) ref25_apply<float, 1>(y0, y1, d0, d1, X, bB[0], c);
-                        else symi_apply<float, 1>(y0, y1, d0, d1, X, bB, K.xoff, c);
+                        if (OPHI == OP_REF25) ref25_apply<float, 1, BOX>(y0, y1, d0, d1, X, bB[0], c);
+                        else symi_apply<float, 1, BOX>(y0, y1, d0, d1, X, bB, K.xoff, c);
                         jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0),
                                 go + P, 1);
                     }
                 }
             }
             __syncwarp();
-            // band rows whose last use was this super-step
-            release_bands_to(kSymBand ? j - 2 : (two ? j : j - 1));
-        } else {
-            __syncwarp();
-            if (!kSymBand) release_bands_to(bwait);  // rows v0-2, v0-1: unused by ref25
+            // band steps read for the last time: j-4, j-3 (symmetric store)
+            // and, at the last super-step, the rest
+            if (kSymBand) {
+                release_rec(bw0);
+                release_rec(bw1);
+                if (j + 2 >= nsteps) {
+                    release_rec(bw2);
+                    if (second) release_rec(bw3);
+                }
+            } else {
+                release_rec(bw2);
+                if (second) release_rec(bw3);
+            }
         }
     }
     __syncwarp();
-    release_bands_to(nband);
 }
 
 // The unit of CTA b after a re-deal (run by one warp; lane 0 writes out[]):
@@ -676,6 +718,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
 // hi}; img = -1 when b gets no work.  Every CTA computes the same partition.
 __device__ __noinline__ void batch_redeal(const SolverArgs& A, int b, int G, int* out)
 {
+    const int kStrip = A.strip;
     const int lane = threadIdx.x & 31;
     auto running = [&](int k) { return __ldcg(A.img_done + k) == 0; };
     int maxT = 0;
@@ -736,17 +779,18 @@ __device__ __noinline__ void batch_redeal(const SolverArgs& A, int b, int G, int
     for (int q = 0; q < 9; ++q) out[q] = res[q];
 }
 
-// Resident CTAs per SM the register budget is sized for: 3 for the 2-byte
-// symmetric stores with shallow rings (their shared memory allows 3), 1 (no
-// register cap) for the other configurations, which shared memory limits to 2.
+// Resident CTAs per SM the register budget is sized for: 3 (4 with
+// 128-column strips) for the 2-byte symmetric stores with shallow rings, as
+// their shared memory allows; 1 (no register cap) for the other
+// configurations, which shared memory limits to 2.
 template <class TLo, int OPLO, int CFG>
 constexpr int solver_min_blocks()
 {
-    return (OPLO == OP_SYMD && sizeof(TLo) == 2 && CFG == 0) ? 3 : 1;
+    return (OPLO == OP_SYMD && sizeof(TLo) == 2 && CFG != 1) ? cfg_cps(CFG) : 1;
 }
 
 template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, bool BATCH>
-__global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
+__global__ void __launch_bounds__(cfg_threads(CFG), solver_min_blocks<TLo, OPLO, CFG>())
     solver_kernel(const __grid_constant__ SolverArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -776,7 +820,7 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
         const int unit = blockIdx.x;
         if (unit < A.nunits) {
             const int st = unit % A.nstrips, sg = unit / A.nstrips;
-            u0 = st * kStrip;
+            u0 = st * cfg_strip(CFG);
             v0 = (int)((long long)A.H * sg / A.nseg);
             v1 = (int)((long long)A.H * (sg + 1) / A.nseg);
         }
@@ -786,9 +830,11 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
     if (tid == 0) {
         for (int i = 0; i < kRvMax + kRbMax; ++i) {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], kConsumers);
+            // vector slots: one arrival per consumer warp; band slots: two
+            // per consumer warp (see run_sweep)
+            mbar_init(&empty[i], i < kRvMax ? cfg_ncol(CFG) : 2 * cfg_ncol(CFG));
         }
-        *reinterpret_cast<volatile int*>(smem + L.red_off + kRedBytes) = 0;
+        *reinterpret_cast<volatile int*>(smem + L.red_off + cfg_red_bytes(CFG)) = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -801,7 +847,7 @@ __global__ void __launch_bounds__(kThreads, solver_min_blocks<TLo, OPLO, CFG>())
     for (int piece = 0; piece < (BATCH ? 2 : 1); ++piece) {
         const int pu0 = piece ? u0b : u0, pv0 = piece ? v0b : v0, pv1 = piece ? v1b : v1;
         for (int v = pv0; v < pv1; ++v)
-            for (int cl = tid; cl < kStrip; cl += blockDim.x) {
+            for (int cl = tid; cl < cfg_strip(CFG); cl += blockDim.x) {
                 const int u = pu0 + cl;
                 if (u >= geo.W) continue;
                 const size_t i = (size_t)v * A.P + u;

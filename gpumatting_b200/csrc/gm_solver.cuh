@@ -12,17 +12,32 @@ enum SweepKind { KIND_KRYLOV = 0, KIND_REPLACE = 1, KIND_JACOBI = 2, NKIND = 3 }
 // OP_REF25: the reference's 25 explicit FP32 bands
 enum OpKind { OP_SYMD = 0, OP_SYMI = 1, OP_REF25 = 2 };
 
-constexpr int kConsumers = 3;                    // consumer warps per CTA
-constexpr int kThreads = 32 * (kConsumers + 1);  // + one TMA producer warp
+// Launch configurations (the kernels' CFG template argument).  A CTA owns a
+// strip of kWarpCols * NCOL columns: NCOL consumer warps side by side, each
+// owning 64 columns (two adjacent pixels per lane), plus one TMA producer
+// warp.
+//   CFG  NCOL  strip  CTAs/SM  rings
+//   0    3     192    3        shallow
+//   1    3     192    2        deep
+//   2    2     128    4        shallow
+constexpr int kNumCfg = 3;
+__host__ __device__ constexpr int cfg_ncol(int cfg) { return cfg == 2 ? 2 : 3; }
+__host__ __device__ constexpr int cfg_cps(int cfg) { return cfg == 0 ? 3 : cfg == 1 ? 2 : 4; }
 constexpr int kWarpCols = 64;                    // output columns per consumer warp (2 per lane)
-constexpr int kStrip = kWarpCols * kConsumers;   // strip width (192)
-constexpr int kBox = kStrip + 16;                // TMA box width: strip + 8 columns each side
+__host__ __device__ constexpr int cfg_strip(int cfg) { return kWarpCols * cfg_ncol(cfg); }
+// TMA box width: strip + 8 columns each side (every box x stays 16-byte aligned)
+__host__ __device__ constexpr int cfg_box(int cfg) { return cfg_strip(cfg) + 16; }
+__host__ __device__ constexpr int cfg_threads(int cfg) { return 32 * (cfg_ncol(cfg) + 1); }
+// Operand ring rows (stencil operand of each consumer warp) and own-row ring
+// rows (r or b of the rows being output).
+constexpr int kOpRows = 8;
+constexpr int kOwnRows = 4;
 constexpr int kRingCols = kWarpCols + 4;         // private operand ring: warp columns + 2 each side
 constexpr int kRvMax = 16;                       // vector ring slots
 constexpr int kRbMax = 16;                       // band ring slots
 constexpr int kNPart = 5;                        // FP64 partial sums per CTA per sweep
 // reduction scratch: per-warp sums + grid totals of up to kNPart + 1 values
-constexpr int kRedBytes = (kThreads / 32 + 1) * (kNPart + 1) * 8;
+__host__ __device__ constexpr int cfg_red_bytes(int cfg) { return (cfg_threads(cfg) / 32 + 1) * (kNPart + 1) * 8; }
 
 // Shared-memory carve of one sweep kind.  Everything here is a compile-time
 // function of the operator types, so the hot loop indexes rings with
@@ -37,7 +52,7 @@ struct KindLayout {
     int voff[5];    // offsets of the vector rows inside a vector slot
     int vbytes[5];  // TMA bytes of each vector row (0 = unused)
     int planes;     // band planes loaded per row
-    int pstride;    // bytes between planes inside a band slot (= kBox * elem)
+    int pstride;    // bytes between planes inside a band slot (= box * elem)
     int xoff;       // offset of the extra plane row (diagonal or gamma), -1 none
     int bbytes;     // TMA bytes of one band row (planes + extra)
 };
@@ -47,10 +62,10 @@ __host__ __device__ constexpr int a128(int x) { return (x + 127) & ~127; }
 // Vector rows per step: Krylov r, q, p, x increment, and the diagonal d for
 // the Jacobi preconditioner (symmetric store; loaded only by PCG solves);
 // replacement base (FP64, mixed only), x increment, p, b; Jacobi x, -, -, b.
-__host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize, bool mixed, int Rv, int Rb)
+__host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize, bool mixed, int Rv, int Rb, int box)
 {
     KindLayout K{};
-    const int vb4 = kBox * 4;
+    const int vb4 = box * 4;
     int vb[5] = {0, 0, 0, 0, 0};
     if (kind == KIND_KRYLOV) {
         vb[0] = vb4; vb[1] = vb4; vb[2] = vb4; vb[3] = vb4;
@@ -67,11 +82,11 @@ __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize
     K.vslot = off;
     const bool sym = op != OP_REF25;
     K.planes = sym ? 12 : 25;
-    K.pstride = kBox * esize;
+    K.pstride = box * esize;
     const int pbytes = K.planes * K.pstride;
     K.xoff = sym ? a128(pbytes) : -1;
-    K.bbytes = pbytes + (sym ? kBox * 4 : 0);
-    K.bslot = sym ? a128(K.xoff + kBox * 4) : a128(pbytes);
+    K.bbytes = pbytes + (sym ? box * 4 : 0);
+    K.bslot = sym ? a128(K.xoff + box * 4) : a128(pbytes);
     K.D = Rv - 1;
     K.Rv = Rv;
     K.Rb = Rb;
@@ -80,10 +95,10 @@ __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize
     return K;
 }
 
-// Ring slots per kind for a depth configuration.  A super-step holds two
-// vector slots and (symmetric store) four band slots, so Rv >= 2 and
-// Rb >= 4 (2 for the reference layout) always make progress; extra slots
-// are prefetch.  Config 0 fits three CTAs per SM (mixed FP16/BF16), config 1
+// Ring slots per kind for a configuration.  A super-step holds two vector
+// slots and (symmetric store) four band slots, so Rv >= 2 and Rb >= 4 (2 for
+// the reference layout) always make progress; extra slots are prefetch.
+// Configs 0 and 2 fit three (four) CTAs per SM with a 2-byte store, config 1
 // trades one CTA per SM for rings about twice as deep.
 __host__ __device__ constexpr int rings_v(int kind, int oplo, int cfg)
 {
@@ -111,18 +126,19 @@ __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int ophi, bool mixed, int cfg)
 {
     Layout L{};
+    const int box = cfg_box(cfg), ncol = cfg_ncol(cfg);
     for (int k = 0; k < NKIND; ++k)
         L.k[k] = kind_layout(k, k == KIND_KRYLOV ? oplo : ophi, k == KIND_KRYLOV ? esize_lo : 4, mixed,
-                             rings_v(k, oplo, cfg), rings_b(k, oplo, cfg));
+                             rings_v(k, oplo, cfg), rings_b(k, oplo, cfg), box);
     int cap = 0;
     for (int k = 0; k < NKIND; ++k) cap = imax(cap, L.k[k].bbase + L.k[k].Rb * L.k[k].bslot);
     L.ring_bytes = a128(cap);
     L.pring_off = L.ring_bytes;
-    L.rring_off = L.pring_off + a128(kConsumers * 8 * kRingCols * ring_esize(mixed));
-    L.full_off = L.rring_off + a128(kConsumers * 4 * kWarpCols * 4);
+    L.rring_off = L.pring_off + a128(ncol * kOpRows * kRingCols * ring_esize(mixed));
+    L.full_off = L.rring_off + a128(ncol * kOwnRows * kWarpCols * 4);
     L.empty_off = L.full_off + a128((kRvMax + kRbMax) * 8);
     L.red_off = L.empty_off + a128((kRvMax + kRbMax) * 8);
-    L.total = L.red_off + a128(kRedBytes + 16);  // + abort flag
+    L.total = L.red_off + a128(cfg_red_bytes(cfg) + 16);  // + abort flag at red_off + cfg_red_bytes
     return L;
 }
 
@@ -186,6 +202,7 @@ struct SolverArgs {
     int P;                    // pitch (elements) of the work vectors
     int W, H;
     int nstrips, nseg, nunits;
+    int strip;                // strip width of the configuration (columns)
     double* partials;         // [2][kNPart][grid]
     GridBarrier* gb;
     SolverOut* out;

@@ -284,8 +284,12 @@ typedef struct gm_solve_params_s {
     float omega;          /* Jacobi damping                                */
     int use_low;          /* mixed store: 1 = iterate with the low-precision planes */
     double timeout_s;     /* limit on any single wait inside the kernel     */
-    int ctas_per_sm;      /* 0 = auto                                      */
-    int strip_width;      /* reserved, ignored: the fused solver's strips are 192 columns */
+    int ctas_per_sm;      /* fused solver CTAs per SM: 0 = auto (as many as fit);
+                             2 selects the deep-ring variant of 192-column
+                             strips for FP16/BF16 stores                   */
+    int strip_width;      /* fused solver strip width in columns: 0 = auto
+                             (192), 192, or 128 (FP16/BF16 stores; up to 4
+                             CTAs per SM)                                  */
     int inject;           /* test hook, 0 in normal use: 1 = the first grid barrier
                              waits for one arrival that never comes, so the call
                              must end with GM_ERR_TIMEOUT after timeout_s */

@@ -20,6 +20,8 @@ relative residual 1e-6.
   solvers (N=1, rank 0) CG, steepest descent and Jacobi to 1e-6, mixed and
           plain, and CG / Jacobi PCG / multigrid PCG to 1e-10 (alpha within
           1e-4 of FP64).
+  slab    (N=1, rank 0) the row-slab split of the same image, its slabs held
+          by one process on this GPU (gpumatting_b200/slab.py).
 
 Multi-GPU: one process per GPU (torchrun); every rank solves its own image
 (seed = rank), no data-path collective; time is the max over ranks.
@@ -551,6 +553,8 @@ def run_ours(args):
         line["large"] = supplementary("large", lambda: run_large(args, stream, peaks))
     if rank == 0 and world == 1 and args.spmv_size > 0:
         line["spmv"] = supplementary("spmv", lambda: run_spmv(args, stream, peaks))
+    if rank == 0 and world == 1 and args.slabs:
+        line["slab"] = supplementary("slab", lambda: run_slab(args, prob, img_d, scr_d, stream))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sweeps = calibrate_sweeps(prob, args.cpu_seconds)
         times, kind, asm = reference_cpu_path(prob, sweeps, 1, steps=1)
@@ -684,6 +688,40 @@ def run_large(args, stream, peaks) -> dict:
                     f"{key}_rel_residual": ra.rel_residual, f"{key}_solve_kernel_ms": ra.kernel_ms,
                     f"{key}_backprop_ms": e0.elapsed_time(e1) - ra.kernel_ms,
                     f"{key}_dimage_finite": bool(torch.isfinite(dimage).all().item())})
+    return out
+
+
+def run_slab(args, prob, img_d, scr_d, stream) -> dict:
+    """The row-slab split of the headline image (gpumatting_b200/slab.py) on
+    this one GPU: the image cut into `n` slabs held by one process, halo rows
+    copied on the device, the slab CG (one operator pass and one FP64
+    reduction per iteration) to rel-res 1e-6 from alpha = 0.5.  On several
+    GPUs each slab would sit on its own GPU and the halo rows travel by NCCL
+    send/recv; here the figure is the data plane's cost per iteration."""
+    import torch
+
+    from gpumatting_b200 import slab as S
+
+    W, H = prob.W, prob.H
+    out = {"workload": f"{W}x{H} headline image, FP32 slab stores, slab CG to rel-res 1e-6 from alpha = 0.5, "
+                       "all slabs on this GPU (halo rows copied on the device)"}
+    for n in args.slabs:
+        slabs = [S.LevinSlab(img_d, scr_d, prob.eps, 100.0, *S.slab_bounds(H, n, k)) for k in range(n)]
+        bs = [sl.rhs() for sl in slabs]
+        comm = S.SlabComm(n, 0, n)
+        xs = [torch.full((sl.R, W), 0.5, device=img_d.device) for sl in slabs]
+        S.slab_cg(slabs, comm, xs, bs, rtol=0.0, max_iters=20)  # warm-up
+        xs = [torch.full((sl.R, W), 0.5, device=img_d.device) for sl in slabs]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = S.slab_cg(slabs, comm, xs, bs, rtol=1e-6, max_iters=5000)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[f"slabs_{n}"] = {"ms": ms, "iters": res.iters, "replacements": res.replacements,
+                             "rel_residual": res.rel_residual, "status": res.status,
+                             "ms_per_iter": ms / max(1, res.iters)}
     return out
 
 
@@ -977,6 +1015,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--spmv-size", type=int, default=4096, help="standalone SpMV measurement size (0 = skip)")
     ap.add_argument("--spmv-reps", type=int, default=20)
+    ap.add_argument("--slabs", type=int, nargs="*", default=[2],
+                    help="row-slab section: slab counts to run on this GPU (empty = skip)")
     ap.add_argument("--spmv-only", action="store_true", help="profiling: only the standalone SpMV passes")
     ap.add_argument("--batch-count", type=int, default=64, help="batched-solve measurement: images (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=3)

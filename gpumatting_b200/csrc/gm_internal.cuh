@@ -151,42 +151,68 @@ __device__ __forceinline__ int ld_volatile_int(const int* p)
 // error any CTA raised (GM_ERR_TIMEOUT from a wait that hit its limit, or a
 // solver status); every wait also returns once it is set.
 struct GridBarrier {
-    unsigned count;
-    unsigned gen;
+    unsigned long long count;  // arrivals so far in this launch (only grows)
     int abort;
     int where;  // which wait gave up: 1 = grid barrier, 2 = TMA row wait
 };
 
+__device__ __forceinline__ unsigned long long atom_add_release_u64(unsigned long long* p, unsigned long long v)
+{
+    unsigned long long old;
+    asm volatile("atom.release.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Arrival half of the grid barrier, run by one thread per CTA.  The arrival
+// counter only grows during a launch (it is zeroed before the launch): an
+// arrival whose atomic returns `old` belongs to round old / G, which is
+// complete once the count reaches (old / G + 1) * G, and `extra` more
+// arrivals are awaited on top of that (the test hook's arrival that never
+// comes).  Every CTA arrives once per round, so no CTA can start round k+1
+// before the round-k arrival of every other CTA has landed.  The atomic's
+// release covers every write the CTA made before the caller's
+// __syncthreads; the acquire loads of the spin order the caller's later
+// reads after all of them.  Compared with a last-arriver flag this saves the
+// last arrival's round trip and the flag store (4.2 -> 3.0 us per barrier and
+// all-reduce with 440 CTAs).  Returns 0 when the wait was abandoned (limit
+// reached or abort set by any CTA).
+__device__ __forceinline__ int grid_arrive_wait(GridBarrier* gb, unsigned G, uint64_t limit_ns, unsigned extra = 0u)
+{
+    const unsigned long long old = atom_add_release_u64(&gb->count, 1ull);
+    const unsigned long long target = (old / G + 1ull) * G + extra;
+    uint64_t t0 = 0;
+    unsigned spins = 0;
+    while (ld_acquire_u64(&gb->count) < target) {
+        ++spins;
+        if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) return 0;
+        if ((spins & 63u) == 0) {
+            const uint64_t now = globaltimer_ns();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > limit_ns) {
+                atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
+                atomicExch(&gb->where, 1);
+                return 0;
+            }
+        }
+    }
+    return 1;
+}
+
 // All CTAs of the grid call this the same number of times.  Returns false
 // when the barrier was abandoned (limit reached or abort set by any CTA).
-__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, uint64_t limit_ns)
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned G, uint64_t limit_ns, unsigned extra = 0u)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int ok = 1;
-        unsigned g = ld_acquire(&gb->gen);
-        __threadfence();
-        unsigned arrived = atomicAdd(&gb->count, 1u);
-        if (arrived == nblocks - 1) {
-            gb->count = 0;
-            __threadfence();
-            st_release(&gb->gen, g + 1);
-        } else {
-            uint64_t t0 = globaltimer_ns();
-            unsigned spins = 0;
-            while (ld_acquire(&gb->gen) == g) {
-                if (ld_volatile_int(&gb->abort)) { ok = 0; break; }
-                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) {
-                    atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
-                    atomicExch(&gb->where, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __threadfence();
+        int ok = grid_arrive_wait(gb, G, limit_ns, extra);
         if (ld_volatile_int(&gb->abort)) ok = 0;
         s_ok = ok;
     }
@@ -322,37 +348,6 @@ __device__ __forceinline__ double warp_sum_range(const double* p, int lo, int hi
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
     return __shfl_sync(0xffffffffu, x, 0);
-}
-
-// Arrival half of the grid barrier, run by one thread: publish nothing more,
-// arrive with an acquire-release atomic (its release covers every write the
-// CTA made before the caller's __syncthreads), and spin on the generation
-// with acquire loads.  Returns 0 when the wait was abandoned.
-__device__ __forceinline__ int grid_arrive_wait(GridBarrier* gb, unsigned G, uint64_t limit_ns)
-{
-    const unsigned g = ld_acquire(&gb->gen);
-    const unsigned arrived = atom_add_acq_rel(&gb->count, 1u);
-    if (arrived == G - 1) {
-        gb->count = 0;
-        st_release(&gb->gen, g + 1);
-        return 1;
-    }
-    uint64_t t0 = 0;
-    unsigned spins = 0;
-    while (ld_acquire(&gb->gen) == g) {
-        ++spins;
-        if ((spins & 7u) == 0 && ld_volatile_int(&gb->abort)) return 0;
-        if ((spins & 63u) == 0) {
-            const uint64_t now = globaltimer_ns();
-            if (t0 == 0) t0 = now;
-            else if (now - t0 > limit_ns) {
-                atomicCAS(&gb->abort, 0, (int)GM_ERR_TIMEOUT);
-                atomicExch(&gb->where, 1);
-                return 0;
-            }
-        }
-    }
-    return 1;
 }
 
 // Grid barrier fused with a deterministic all-reduce of NV doubles per

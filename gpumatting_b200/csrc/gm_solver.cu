@@ -864,7 +864,7 @@ __global__ void __launch_bounds__(cfg_threads(CFG), solver_min_blocks<TLo, OPLO,
             }
     }
     const unsigned G = gridDim.x;
-    bool ok = grid_sync(A.gb, G + (A.inject == 1 ? 1u : 0u), A.limit_ns);
+    bool ok = grid_sync(A.gb, G, A.limit_ns, A.inject == 1 ? 1u : 0u);
 
     int status = GM_OK, it = 0, nrep = 0, parity = 0;
     int kind = jac ? KIND_JACOBI : KIND_REPLACE;

@@ -81,3 +81,37 @@ def test_compute_error_gpu(orc):
     gt = rng.uniform(0, 1, size=(41, 37)).astype(np.float32)
     v = api.compute_error(torch.from_numpy(al).cuda(), torch.from_numpy(gt).cuda(), 37, 41)
     assert abs(v - orc.compute_error(al, gt)) <= 1e-12
+
+
+@pytest.mark.parametrize("rows", [1_000_003, 4096 * 64])
+def test_banded_product_four_row_path_matches_one_row_path(rows):
+    """gm_bm_ax / gm_bm_axpy take four rows per thread with 128-bit band loads
+    when the planes are 16-byte aligned with a pitch of a multiple of 4
+    floats, and one row per thread otherwise; both sum every row in band
+    order, so the results agree bit for bit (rows % 4 != 0 covers the tail)."""
+    torch = torch_cuda()
+    from gpumatting_b200 import api
+
+    W = 4096
+    offs = [du + W * dv for dv in range(-2, 3) for du in range(-2, 3)]
+    rng = np.random.default_rng(rows)
+    a = rng.standard_normal((25, rows)).astype(np.float32)
+    pad = 2 * W + 2
+    xh = rng.standard_normal(rows).astype(np.float32)
+    x = api.PaddedVector(rows, pad, xh)
+    yv = torch.from_numpy(rng.standard_normal(rows).astype(np.float32)).cuda()
+    outs = []
+    for apitch in (None, rows + 1):  # aligned pitch (four-row path), odd pitch (one-row path)
+        Lm = api.DeviceBandedMatrix.from_host(a, offs, apitch)
+        b = torch.empty(rows, dtype=torch.float32, device="cuda")
+        api.bm_ax(b, Lm, x)
+        c = torch.empty(rows, dtype=torch.float32, device="cuda")
+        api.bm_axpy(c, Lm, x, yv, add=False)
+        outs.append((b.cpu().numpy(), c.cpu().numpy()))
+    for u, v in zip(*outs):
+        assert np.array_equal(u.view(np.uint32), v.view(np.uint32))
+    xs = np.zeros(rows + 2 * pad)
+    xs[pad:pad + rows] = xh
+    i = rng.integers(0, rows, 2000)
+    ref = sum(a[j, i].astype(np.float64) * xs[pad + i + offs[j]] for j in range(25))
+    assert np.abs(outs[0][0][i] - ref).max() <= 1e-4 * (1 + np.abs(ref).max())

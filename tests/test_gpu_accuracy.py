@@ -134,6 +134,19 @@ def test_1080p_tight_solve_within_1e4_of_fp64(hd, solver):
     assert err <= TOL
 
 
+@pytest.mark.parametrize("prec,solver", [("bf16", "cg"), ("bf16", "mg"), ("fp32", "cg"), ("fp32", "pcg")])
+def test_1080p_other_stores_within_1e4_of_fp64(hd, prec, solver):
+    """BF16 and FP32 stores at the headline size: their FP64 replacement runs
+    on the FP32 planes too, so at rel-res 1e-10 they also land within 1e-4
+    of the FP64 solution."""
+    p, g, gam, b, _ = hd
+    _, res, x = _solve(p, prec, solver, 1e-10)
+    assert res.status == 0 and res.rel_residual <= 1e-10, res
+    err = float(np.abs(_sampled(g, x) - g["alpha64"]).max())
+    print(f"1080p {prec} {solver} rel-res 1e-10: {res.iters} it, alpha max-abs vs FP64 {err:.2e}")
+    assert err <= TOL
+
+
 def test_1080p_rel_res_1e6_as_accurate_as_fp64_cg(hd):
     p, g, gam, b, st = hd
     _, res, x = _solve(p, "fp16", "cg", 1e-6, st=st)

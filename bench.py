@@ -697,7 +697,8 @@ def run_slab(args, prob, img_d, scr_d, stream) -> dict:
     copied on the device, the slab CG (one operator pass and one FP64
     reduction per iteration) to rel-res 1e-6 from alpha = 0.5.  On several
     GPUs each slab would sit on its own GPU and the halo rows travel by NCCL
-    send/recv; here the figure is the data plane's cost per iteration."""
+    send/recv; here the figure is the data plane's cost per iteration (the
+    scalars on the device, chunks of 10 iterations as one CUDA graph)."""
     import torch
 
     from gpumatting_b200 import slab as S
@@ -710,7 +711,7 @@ def run_slab(args, prob, img_d, scr_d, stream) -> dict:
         bs = [sl.rhs() for sl in slabs]
         comm = S.SlabComm(n, 0, n)
         xs = [torch.full((sl.R, W), 0.5, device=img_d.device) for sl in slabs]
-        S.slab_cg(slabs, comm, xs, bs, rtol=0.0, max_iters=20)  # warm-up
+        S.slab_cg(slabs, comm, xs, bs, rtol=0.0, max_iters=60)  # warm-up (captures the chunk graph)
         xs = [torch.full((sl.R, W), 0.5, device=img_d.device) for sl in slabs]
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -103,6 +103,10 @@ SIGNATURES = {
     "gm_levin_band_offsets": (None, [_i, C.POINTER(C.c_int)]),
     "gm_levin_pad": (_i, [_i]),
     "gm_compute_error": (_i, [C.POINTER(C.c_double), _vp, _vp, _i, _i, _vp]),
+    "gm_cg_dots4": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "gm_cg_update": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _i, _vp]),
+    "gm_cg_scalars": (_i, [_vp, _vp, _vp, _vp]),
+    "gm_cg_update_dev": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _i, _i, _vp, _vp]),
     "gm_levin_store_alloc": (_i, [C.POINTER(GmLevinStore), _i, _i, _i]),
     "gm_levin_store_free": (_i, [C.POINTER(GmLevinStore)]),
     "gm_levin_assemble": (_i, [C.POINTER(GmLevinStore), C.POINTER(GmImage), C.POINTER(GmScribbles), _d,

@@ -246,6 +246,73 @@ def compute_error(alpha, gt, W: int, H: int, stream=None) -> float:
     return v.value
 
 
+def _row_blocks(*ts):
+    """(rows, W, pitches) of equally shaped [rows, W] float32 CUDA blocks
+    whose rows are contiguous (a row pitch of stride(0) floats)."""
+    torch = _torch()
+    t0 = ts[0]
+    for t in ts:
+        if not isinstance(t, torch.Tensor) or t.dtype != torch.float32:
+            raise TypeError("operands must be float32 torch tensors")
+        if not t.is_cuda or t.device != t0.device:
+            raise ValueError("operands must be CUDA tensors on one device")
+        if t.dim() != 2 or t.shape != t0.shape:
+            raise ValueError(f"operands must be [rows, W] blocks of one shape (got {[tuple(u.shape) for u in ts]})")
+        if t.shape[1] > 1 and t.stride(1) != 1:
+            raise ValueError("rows must be contiguous")
+        if t.stride(0) < t.shape[1] or t.stride(0) > 2**31 - 1:
+            raise ValueError("row pitch out of range")
+    return int(t0.shape[0]), int(t0.shape[1]), [max(int(t.stride(0)), int(t.shape[1])) for t in ts]
+
+
+def cg_dots4(r, p, q, out=None, stream=None):
+    """FP64 [r.r, p.q, r.q, q.q] over [rows, W] row blocks, into the device
+    tensor `out` (4 doubles; allocated when None)."""
+    torch = _torch()
+    rows, W, (rp, pp, qp) = _row_blocks(r, p, q)
+    if out is None:
+        out = torch.empty(4, dtype=torch.float64, device=r.device)
+    if out.dtype != torch.float64 or out.device != r.device or out.numel() < 4 or not out.is_contiguous():
+        raise TypeError("out must be a contiguous float64 tensor of 4 elements on the operands' device")
+    L.check(L.load().gm_cg_dots4(out.data_ptr(), r.data_ptr(), rp, p.data_ptr(), pp, q.data_ptr(), qp, W, rows,
+                                 _stream(stream)))
+    return out
+
+
+def cg_update(x, r, p, q, alpha: float, beta: float, update_p: bool = True, stream=None):
+    """x += alpha p; r -= alpha q; then p = r + beta p when update_p (FP32)."""
+    rows, W, (xp, rp, pp, qp) = _row_blocks(x, r, p, q)
+    L.check(L.load().gm_cg_update(x.data_ptr(), xp, r.data_ptr(), rp, p.data_ptr(), pp, q.data_ptr(), qp, W, rows,
+                                  float(alpha), float(beta), 1 if update_p else 0, _stream(stream)))
+
+
+def _f64_dev(t, n: int, name: str, device):
+    torch = _torch()
+    if (not isinstance(t, torch.Tensor) or t.dtype != torch.float64 or t.device != device or t.numel() < n
+            or not t.is_contiguous()):
+        raise TypeError(f"{name} must be a contiguous float64 tensor of {n} elements on {device}")
+
+
+def cg_scalars(coef, state, sums4, stream=None):
+    """One thread on the device: coef = [alpha, beta, mode] from the summed
+    sums4 = [r.r, p.q, r.q, q.q], advancing the 6-double device state
+    (threshold, r.r, next r.r, iterations, stop code, stop-at count)."""
+    _f64_dev(sums4, 4, "sums4", sums4.device)
+    _f64_dev(coef, 3, "coef", sums4.device)
+    _f64_dev(state, 6, "state", sums4.device)
+    if not sums4.is_cuda:
+        raise ValueError("cg_scalars needs CUDA tensors")
+    L.check(L.load().gm_cg_scalars(coef.data_ptr(), state.data_ptr(), sums4.data_ptr(), _stream(stream)))
+
+
+def cg_update_dev(x, r, p, q, coef, stream=None):
+    """cg_update with [alpha, beta, mode] read from the device tensor coef."""
+    rows, W, (xp, rp, pp, qp) = _row_blocks(x, r, p, q)
+    _f64_dev(coef, 3, "coef", x.device)
+    L.check(L.load().gm_cg_update_dev(x.data_ptr(), xp, r.data_ptr(), rp, p.data_ptr(), pp, q.data_ptr(), qp, W,
+                                      rows, coef.data_ptr(), _stream(stream)))
+
+
 # ---------------------------------------------------------------------------
 # Native: symmetric Levin store
 # ---------------------------------------------------------------------------

@@ -2,6 +2,8 @@
 #include <stdarg.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "gm_internal.cuh"
 
 static thread_local char g_msg[1024] = "";
@@ -26,6 +28,80 @@ int gm_note_status(int s)
 extern "C" int gm_last_status(void) { return g_status; }
 extern "C" const char* gm_last_error(void) { return g_msg; }
 extern "C" const char* gm_version(void) { return "gpumatting_b200 0.1 (sm_100a)"; }
+
+// The driver's identifier of the current context (unique for the life of
+// the process, never reused), or 0 when the driver cannot say.
+unsigned long long gm_context_id()
+{
+    typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+    typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrentFn)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)p;
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
+
+// Stream-ordered scratch for the small per-call buffers (reduction partials).
+// The device's default memory pool hands freed memory back to the driver at
+// every synchronisation (release threshold 0), so a caller that synchronises
+// between calls -- a host-driven iteration that reads each dot product --
+// would pay a fresh mapping on every call.  A pool owned by the library, one
+// per device and context, with a 64 MiB release threshold keeps these
+// buffers mapped.  Under stream capture, or when the context id is unknown,
+// the default pool is used.
+static cudaMemPool_t scratch_pool()
+{
+    constexpr int kMaxDevices = 64;
+    struct Entry { unsigned long long ctx; cudaMemPool_t pool; };
+    static std::mutex mu;
+    static Entry cache[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    const unsigned long long ctx = gm_context_id();
+    if (ctx == 0) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    Entry& e = cache[dev];
+    if (e.pool && e.ctx == ctx) return e.pool;
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    uint64_t keep = 64ull << 20;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    e.ctx = ctx;
+    e.pool = pool;
+    return pool;
+}
+
+cudaError_t gm_scratch_alloc(void** p, size_t bytes, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusActive;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+        if (cudaMemPool_t pool = scratch_pool()) return cudaMallocFromPoolAsync(p, bytes, pool, st);
+    }
+    cudaGetLastError();
+    return cudaMallocAsync(p, bytes, st);
+}
 
 int gm_check_device(int* sm_count)
 {

@@ -38,6 +38,14 @@ void gm_set_error_msg(const char* fmt, ...);
 // otherwise.
 int gm_check_device(int* sm_count);
 
+// The driver's identifier of the current context (unique for the life of
+// the process, never reused), or 0 when the driver cannot say.
+unsigned long long gm_context_id();
+
+// Stream-ordered scratch from a library-owned pool that stays mapped across
+// synchronisations (free with cudaFreeAsync).
+cudaError_t gm_scratch_alloc(void** p, size_t bytes, cudaStream_t st);
+
 // ---------------------------------------------------------------------------
 // Tensor maps
 // ---------------------------------------------------------------------------

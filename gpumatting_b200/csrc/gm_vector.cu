@@ -123,7 +123,7 @@ static int inner_prod_impl(float* rf, double* rd, const float* x, const float* y
     if (!x || !y) { gm_set_error_msg("NULL vector"); return GM_ERR_INVALID; }
     const int nb = dot_blocks(len);
     double* scratch = nullptr;
-    GM_CUDA_TRY(cudaMallocAsync((void**)&scratch, sizeof(double) * nb, st));
+    GM_CUDA_TRY(gm_scratch_alloc((void**)&scratch, sizeof(double) * nb, st));
     int rc = dot_with_scratch(x, y, len, scratch, nb, rf, rd, st);
     cudaFreeAsync(scratch, st);
     return rc;
@@ -150,7 +150,7 @@ extern "C" int gm_compute_error(double* mse_host, const float* alpha, const floa
     const int n = W * H;
     const int nb = dot_blocks(n);
     double* scratch = nullptr;
-    GM_CUDA_TRY(cudaMallocAsync((void**)&scratch, sizeof(double) * (nb + 1), st));
+    GM_CUDA_TRY(gm_scratch_alloc((void**)&scratch, sizeof(double) * (nb + 1), st));
     mse_partial_kernel<<<nb, kVecThreads, 0, st>>>(alpha, gt, n, scratch);
     dot_finish_kernel<<<1, 32, 0, st>>>(scratch, nb, nullptr, scratch + nb);
     double ssd = 0.0;
@@ -215,6 +215,217 @@ extern "C" void computeError(float* alpha, float* gtAlpha, int imW, int imH)
     if (rc == GM_OK) printf("Ground truth MSE: %.3e\n", mse);
 }
 
+// ---- CG building blocks over pitched row blocks (the row-slab solver) ----
+//
+// A host-driven CG over one slab of rows (the slab split of one image over
+// several GPUs) needs, per iteration, the four FP64 sums of the single-
+// reduction recurrence and one elementwise update; each is one launch here
+// (plus a one-warp pass that adds the per-block sums in block order, so the
+// sums are deterministic).  Rows are `rows` runs of W floats, `pitch` floats
+// apart.
+namespace gm {
+
+constexpr int kCgThreads = 256;
+
+__global__ void cg_dots4_kernel(const float* __restrict__ r, int rp, const float* __restrict__ p, int pp,
+                                const float* __restrict__ q, int qp, int W, int rows, double* part)
+{
+    __shared__ double red[32 * 4];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long i = blockIdx.x; i < rows; i += gridDim.x) {
+        const float* ri = r + i * rp;
+        const float* pi = p + i * pp;
+        const float* qi = q + i * qp;
+        for (int j = threadIdx.x; j < W; j += blockDim.x) {
+            const double rv = ri[j], pv = pi[j], qv = qi[j];
+            acc[0] += rv * rv;
+            acc[1] += pv * qv;
+            acc[2] += rv * qv;
+            acc[3] += qv * qv;
+        }
+    }
+    block_sum<4>(acc, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) part[(size_t)k * gridDim.x + blockIdx.x] = acc[k];
+}
+
+__global__ void cg_dots4_finish(const double* part, int nb, double* out)
+{
+    __shared__ double red[32 * 4];
+    double t[4];
+    grid_total<4>(part, nb, t, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) out[k] = t[k];
+}
+
+// x += alpha p; r -= alpha q; then (update_p) p = r + beta p.
+__global__ void cg_update_kernel(float* __restrict__ x, int xp, float* __restrict__ r, int rp, float* __restrict__ p,
+                                 int pp, const float* __restrict__ q, int qp, int W, int rows, float alpha, float beta,
+                                 int update_p)
+{
+    for (long long i = blockIdx.x; i < rows; i += gridDim.x) {
+        float* xi = x + i * xp;
+        float* ri = r + i * rp;
+        float* pi = p + i * pp;
+        const float* qi = q + i * qp;
+        for (int j = threadIdx.x; j < W; j += blockDim.x) {
+            const float pv = pi[j];
+            xi[j] += alpha * pv;
+            const float rn = ri[j] - alpha * qi[j];
+            ri[j] = rn;
+            if (update_p) pi[j] = rn + beta * pv;
+        }
+    }
+}
+
+// Device-side scalars of one iteration (one thread).  state: [0] threshold
+// on the recurrence's next r.r (< 0: none), [1] r.r of this iteration, [2]
+// the recurrence's next r.r, [3] iterations taken, [4] stop code, [5] the
+// iteration count at which to stop for a residual replacement.  coef: alpha,
+// beta, mode (0 nothing, 1 x and r, 2 x, r and p).
+__global__ void cg_scalars_kernel(double* coef, double* state, const double* sums)
+{
+    double mode = 0.0, alpha = 0.0, beta = 0.0;
+    if (state[4] == 0.0) {
+        const double rr = sums[0], pq = sums[1], rq = sums[2], qq = sums[3];
+        if (!(pq > 0.0) || rr != rr) {
+            state[4] = 2.0;
+        } else {
+            alpha = rr / pq;
+            const double nx = fmax(rr - 2.0 * alpha * rq + alpha * alpha * qq, 0.0);
+            const double it = state[3] + 1.0;
+            state[1] = rr;
+            state[2] = nx;
+            state[3] = it;
+            if ((state[0] >= 0.0 && nx <= state[0]) || it >= state[5]) {
+                state[4] = 1.0;
+                mode = 1.0;
+            } else {
+                beta = nx / rr;
+                mode = 2.0;
+            }
+        }
+    }
+    coef[0] = alpha;
+    coef[1] = beta;
+    coef[2] = mode;
+}
+
+// gm_cg_update with the coefficients read from the device.
+__global__ void cg_update_dev_kernel(float* __restrict__ x, int xp, float* __restrict__ r, int rp,
+                                     float* __restrict__ p, int pp, const float* __restrict__ q, int qp, int W,
+                                     int rows, const double* __restrict__ coef)
+{
+    const double mode = coef[2];
+    if (mode == 0.0) return;
+    const float alpha = (float)coef[0], beta = (float)coef[1];
+    const bool update_p = mode == 2.0;
+    for (long long i = blockIdx.x; i < rows; i += gridDim.x) {
+        float* xi = x + i * xp;
+        float* ri = r + i * rp;
+        float* pi = p + i * pp;
+        const float* qi = q + i * qp;
+        for (int j = threadIdx.x; j < W; j += blockDim.x) {
+            const float pv = pi[j];
+            xi[j] += alpha * pv;
+            const float rn = ri[j] - alpha * qi[j];
+            ri[j] = rn;
+            if (update_p) pi[j] = rn + beta * pv;
+        }
+    }
+}
+
+static int cg_blocks(int rows)
+{
+    int nsm = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return rows < 4 * nsm ? (rows > 0 ? rows : 1) : 4 * nsm;
+}
+
+static int check_block(const void* a, int pitch, int W, const char* name)
+{
+    if (!a || pitch < W) {
+        gm_set_error_msg("%s: NULL or pitch %d < W %d", name, pitch, W);
+        return GM_ERR_INVALID;
+    }
+    return GM_OK;
+}
+
+}  // namespace gm
+
+extern "C" int gm_cg_dots4(double* out4, const float* r, int r_pitch, const float* p, int p_pitch, const float* q,
+                           int q_pitch, int W, int rows, void* stream)
+{
+    if (!out4 || W < 0 || rows < 0) {
+        gm_set_error_msg("gm_cg_dots4: bad arguments");
+        return GM_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((long long)W * rows == 0) {
+        GM_CUDA_TRY(cudaMemsetAsync(out4, 0, 4 * sizeof(double), st));
+        return GM_OK;
+    }
+    GM_TRY(gm::check_block(r, r_pitch, W, "r"));
+    GM_TRY(gm::check_block(p, p_pitch, W, "p"));
+    GM_TRY(gm::check_block(q, q_pitch, W, "q"));
+    const int nb = gm::cg_blocks(rows);
+    double* part = nullptr;
+    GM_CUDA_TRY(gm_scratch_alloc((void**)&part, sizeof(double) * 4 * nb, st));
+    gm::cg_dots4_kernel<<<nb, gm::kCgThreads, 0, st>>>(r, r_pitch, p, p_pitch, q, q_pitch, W, rows, part);
+    gm::cg_dots4_finish<<<1, 128, 0, st>>>(part, nb, out4);
+    cudaFreeAsync(part, st);
+    GM_CUDA_TRY(cudaGetLastError());
+    return GM_OK;
+}
+
+extern "C" int gm_cg_update(float* x, int x_pitch, float* r, int r_pitch, float* p, int p_pitch, const float* q,
+                            int q_pitch, int W, int rows, float alpha, float beta, int update_p, void* stream)
+{
+    if (W < 0 || rows < 0) {
+        gm_set_error_msg("gm_cg_update: bad arguments");
+        return GM_ERR_INVALID;
+    }
+    if ((long long)W * rows == 0) return GM_OK;
+    GM_TRY(gm::check_block(x, x_pitch, W, "x"));
+    GM_TRY(gm::check_block(r, r_pitch, W, "r"));
+    GM_TRY(gm::check_block(p, p_pitch, W, "p"));
+    GM_TRY(gm::check_block(q, q_pitch, W, "q"));
+    gm::cg_update_kernel<<<gm::cg_blocks(rows), gm::kCgThreads, 0, (cudaStream_t)stream>>>(
+        x, x_pitch, r, r_pitch, p, p_pitch, q, q_pitch, W, rows, alpha, beta, update_p);
+    GM_CUDA_TRY(cudaGetLastError());
+    return GM_OK;
+}
+
+extern "C" int gm_cg_scalars(double* coef, double* state, const double* sums4, void* stream)
+{
+    if (!coef || !state || !sums4) {
+        gm_set_error_msg("gm_cg_scalars: NULL argument");
+        return GM_ERR_INVALID;
+    }
+    gm::cg_scalars_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(coef, state, sums4);
+    GM_CUDA_TRY(cudaGetLastError());
+    return GM_OK;
+}
+
+extern "C" int gm_cg_update_dev(float* x, int x_pitch, float* r, int r_pitch, float* p, int p_pitch,
+                                const float* q, int q_pitch, int W, int rows, const double* coef, void* stream)
+{
+    if (W < 0 || rows < 0 || !coef) {
+        gm_set_error_msg("gm_cg_update_dev: bad arguments");
+        return GM_ERR_INVALID;
+    }
+    if ((long long)W * rows == 0) return GM_OK;
+    GM_TRY(gm::check_block(x, x_pitch, W, "x"));
+    GM_TRY(gm::check_block(r, r_pitch, W, "r"));
+    GM_TRY(gm::check_block(p, p_pitch, W, "p"));
+    GM_TRY(gm::check_block(q, q_pitch, W, "q"));
+    gm::cg_update_dev_kernel<<<gm::cg_blocks(rows), gm::kCgThreads, 0, (cudaStream_t)stream>>>(
+        x, x_pitch, r, r_pitch, p, p_pitch, q, q_pitch, W, rows, coef);
+    GM_CUDA_TRY(cudaGetLastError());
+    return GM_OK;
+}
+
 // ---- allocation-free dot product ----
 //
 // For callers that may not allocate device memory while they run: code that
@@ -232,32 +443,6 @@ __device__ __align__(256) double g_static_dot_parts[kStaticDotParts];
 
 #include <mutex>
 
-// The driver's identifier of the current context (unique for the life of
-// the process, never reused), or 0 when the driver cannot say.
-static unsigned long long current_context_id()
-{
-    typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
-    typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
-    static CtxGetCurrentFn get_current = nullptr;
-    static CtxGetIdFn get_id = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            get_current = (CtxGetCurrentFn)p;
-        p = nullptr;
-        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            get_id = (CtxGetIdFn)p;
-    });
-    CUcontext c = nullptr;
-    unsigned long long id = 0;
-    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
-    return 0;
-}
-
 // Device address of the static partials in the current context of device
 // dev.  Resolved once per context: a cudaDeviceReset (or any new context on
 // the same ordinal) changes the context id and the address is looked up
@@ -269,7 +454,7 @@ static double* static_dot_parts(int dev)
     static std::mutex mu;
     static Entry cache[kMaxDevices] = {};
     if (dev < 0 || dev >= kMaxDevices) return nullptr;
-    const unsigned long long ctx = current_context_id();
+    const unsigned long long ctx = gm_context_id();
     std::lock_guard<std::mutex> lock(mu);
     Entry& e = cache[dev];
     if (!e.addr || ctx == 0 || e.ctx != ctx) {
@@ -279,7 +464,7 @@ static double* static_dot_parts(int dev)
         // has yet); the id is read again once that context exists.
         if (cudaGetSymbolAddress(&p, gm::g_static_dot_parts) != cudaSuccess) return nullptr;
         e.addr = static_cast<double*>(p);
-        e.ctx = current_context_id();
+        e.ctx = gm_context_id();
     }
     return e.addr;
 }

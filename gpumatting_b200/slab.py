@@ -33,8 +33,14 @@ p) and all-reduces four FP64 sums (r.r, p.q, r.q, q.q); alpha = r.r / p.q
 and the next r.r = r.r - 2 alpha r.q + alpha^2 q.q give beta without a second
 reduction.  Every `replace_every` iterations, and before it stops, the true
 residual b - A x (one more exchange and reduction) replaces the recurrence;
-convergence is declared on the true residual only.  With one slab and no
-process group it is an ordinary single-domain CG.  The reference solves one
+convergence is declared on the true residual only.  p lives in the slab's
+extended input buffer, so on the GPU one iteration is the halo exchange, one
+gm_levin_apply, one gm_cg_dots4 (two launches) and one gm_cg_update_dev per
+slab, the sum and all-reduce of four doubles, and one gm_cg_scalars launch
+that turns them into alpha and beta on the device; no vector is copied and
+the host reads the iteration state once per chunk of iterations.  With every
+slab on one rank the chunk is a CUDA graph.  With one slab and no process
+group it is an ordinary single-domain CG.  The reference solves one
 image per process (main.cu:458-526); it has no multi-GPU path.
 """
 from __future__ import annotations
@@ -99,22 +105,35 @@ class SlabComm:
         if self._dist is None:
             return
         dist = self._dist
-        ops = []
+        ops, back = [], []
         first, last = slabs[0], slabs[-1]
-        # whole rows of a contiguous [rows, W] tensor: contiguous views, so the
-        # received rows land in the vector itself
+
+        def send(t):
+            return t if t.is_contiguous() else t.contiguous()
+
+        def recv(t):
+            # a pitched view (a slab buffer wider than W) receives through a
+            # contiguous staging tensor, copied in after the wait
+            if t.is_contiguous():
+                return t
+            tmp = t.new_empty(t.shape)
+            back.append((t, tmp))
+            return tmp
+
         if self.first > 0:
             peer = self._rank_of(self.first - 1)
-            ops.append(dist.P2POp(dist.isend, vecs[0][first.above:2 * first.above], peer, self.group))
-            ops.append(dist.P2POp(dist.irecv, vecs[0][:first.above], peer, self.group))
+            ops.append(dist.P2POp(dist.isend, send(vecs[0][first.above:2 * first.above]), peer, self.group))
+            ops.append(dist.P2POp(dist.irecv, recv(vecs[0][:first.above]), peer, self.group))
         if self.first + self.count < self.nslabs:
             peer = self._rank_of(self.first + self.count)
             lo = last.above + last.R
-            ops.append(dist.P2POp(dist.isend, vecs[-1][lo - last.below:lo], peer, self.group))
-            ops.append(dist.P2POp(dist.irecv, vecs[-1][lo:lo + last.below], peer, self.group))
+            ops.append(dist.P2POp(dist.isend, send(vecs[-1][lo - last.below:lo]), peer, self.group))
+            ops.append(dist.P2POp(dist.irecv, recv(vecs[-1][lo:lo + last.below]), peer, self.group))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
+        for t, tmp in back:
+            t.copy_(tmp)
 
     def allreduce(self, t):
         """Sum of an FP64 tensor over all slabs (in place)."""
@@ -131,77 +150,192 @@ class SlabResult:
     rel_residual: float  # true relative residual over the whole image
 
 
+def _is_cuda(t) -> bool:
+    return bool(getattr(t, "is_cuda", False))
+
+
+def _dots4(r, p, q, out):
+    """out[:] = FP64 [r.r, p.q, r.q, q.q] of one slab's own rows."""
+    if _is_cuda(r):
+        from . import api
+
+        api.cg_dots4(r, p, q, out=out)
+    else:
+        import torch
+
+        rd, pd, qd = r.double(), p.double(), q.double()
+        out.copy_(torch.stack([(rd * rd).sum(), (pd * qd).sum(), (rd * qd).sum(), (qd * qd).sum()]))
+
+
+def _update(x, r, p, q, alpha: float, beta: float, update_p: bool) -> None:
+    """x += alpha p; r -= alpha q; then p = r + beta p when update_p."""
+    if _is_cuda(x):
+        from . import api
+
+        api.cg_update(x, r, p, q, alpha, beta, update_p)
+    else:
+        x.add_(p, alpha=alpha)
+        r.sub_(q, alpha=alpha)
+        if update_p:
+            p.mul_(beta).add_(r)
+
+
+# Device iteration state (6 doubles, the layout gm_cg_scalars keeps).
+_THR, _RR, _RR_NEXT, _ITERS, _STOP, _STOP_AT = range(6)
+
+
+def _scalars(coef, state, sums) -> None:
+    """coef = [alpha, beta, mode] from the summed sums, advancing state:
+    gm_cg_scalars on CUDA tensors, the same rule in Python on CPU ones."""
+    if _is_cuda(sums):
+        from . import api
+
+        api.cg_scalars(coef, state, sums)
+        return
+    st = state.tolist()
+    rr, pq, rq, qq = sums.tolist()
+    alpha = beta = mode = 0.0
+    if st[_STOP] == 0.0:
+        if not (pq > 0.0) or rr != rr:
+            st[_STOP] = 2.0
+        else:
+            alpha = rr / pq
+            nx = max(rr - 2.0 * alpha * rq + alpha * alpha * qq, 0.0)
+            st[_RR], st[_RR_NEXT], st[_ITERS] = rr, nx, st[_ITERS] + 1.0
+            if (st[_THR] >= 0.0 and nx <= st[_THR]) or st[_ITERS] >= st[_STOP_AT]:
+                st[_STOP], mode = 1.0, 1.0
+            else:
+                beta, mode = nx / rr, 2.0
+        state.copy_(state.new_tensor(st))
+    coef.copy_(coef.new_tensor([alpha, beta, mode]))
+
+
+def _update_dev(x, r, p, q, coef) -> None:
+    """The update with [alpha, beta, mode] read from coef."""
+    if _is_cuda(x):
+        from . import api
+
+        api.cg_update_dev(x, r, p, q, coef)
+        return
+    alpha, beta, mode = coef.tolist()
+    if mode != 0.0:
+        _update(x, r, p, q, alpha, beta, mode == 2.0)
+
+
 def slab_cg(slabs, comm: SlabComm, x, b, rtol: float = 1e-6, max_iters: int = 5000,
-            replace_every: int = 50) -> SlabResult:
+            replace_every: int = 50, chunk: int = 10, graph: bool | None = None) -> SlabResult:
     """CG on the whole image from its local slabs.  x[i], b[i]: own-row
     tensors (R_i x W) of local slab i; x holds the initial guess and receives
-    the solution.  Every slab object has .R, .above, .below and
-    .apply(x_ext) -> y_ext on extended (above + R + below) x W tensors."""
+    the solution.  Every slab object has .R, .above, .below, .ext (its
+    extended (above + R + below) x W input vector, which holds the search
+    direction p) and .apply_ext() -> the own rows (R x W) of A ext, a view
+    that stays valid until its next call.
+
+    The scalars of each iteration stay on the device (gm_cg_scalars): the
+    host queues `chunk` iterations and reads the 6-double state once per
+    chunk.  An iteration after the stop (the recurrence met rtol, the next
+    residual replacement is due, or a breakdown) changes nothing, so the
+    iteration count is exact.  graph (CUDA tensors, all slabs on this rank
+    only; None = whenever that holds): the chunk is captured once as a CUDA
+    graph and replayed."""
     import torch
 
     n = len(slabs)
-    ext = [torch.zeros((s.above + s.R + s.below,) + tuple(x[i].shape[1:]), dtype=x[i].dtype, device=x[i].device)
-           for i, s in enumerate(slabs)]
     dev = x[0].device
+    cuda = _is_cuda(x[0])
+    ext = [s.ext for s in slabs]
+    p = [e[s.above:s.above + s.R] for s, e in zip(slabs, ext)]  # own rows of the extended vectors
+    r = [torch.empty_like(b[i]) for i in range(n)]
+    parts = torch.zeros((n, 4), dtype=torch.float64, device=dev)
+    sums = torch.zeros(4, dtype=torch.float64, device=dev)
+    coef = torch.zeros(3, dtype=torch.float64, device=dev)
+    state = torch.zeros(6, dtype=torch.float64, device=dev)
+    local = comm._dist is None or comm._dist.get_world_size(comm.group) == 1
+    if graph is None:
+        graph = cuda and local
+    if graph and not (cuda and local):
+        raise ValueError("graph capture needs CUDA tensors and every slab on this rank")
 
-    def own(i, t):
-        s = slabs[i]
-        return t[s.above:s.above + s.R]
-
-    def apply_all(src):
-        """q_i = own rows of A_i (src with halos)."""
-        for i in range(n):
-            own(i, ext[i]).copy_(src[i])
+    def apply_p():
+        """q_i = own rows of A_i p (halos exchanged first)."""
         comm.exchange(slabs, ext)
-        # (the operator may return a view of its own buffer: copy out)
-        return [own(i, slabs[i].apply(ext[i])).clone() for i in range(n)]
+        return [s.apply_ext() for s in slabs]
 
-    def dots(pairs):
-        """FP64 sums over all slabs of the products of each pair."""
-        acc = torch.zeros(len(pairs), dtype=torch.float64, device=dev)
-        for k, (u, v) in enumerate(pairs):
+    def reduce4(rs, ps, qs):
+        """sums = FP64 [r.r, p.q, r.q, q.q] over all slabs (on the device)."""
+        if n == 1:
+            _dots4(rs[0], ps[0], qs[0], sums)
+        else:
             for i in range(n):
-                acc[k] += torch.sum(u[i].double() * v[i].double())
-        comm.allreduce(acc)
-        return [float(a) for a in acc.tolist()]
+                _dots4(rs[i], ps[i], qs[i], parts[i])
+            torch.sum(parts, dim=0, out=sums)
+        comm.allreduce(sums)
+
+    def iteration():
+        q = apply_p()
+        reduce4(r, p, q)
+        _scalars(coef, state, sums)
+        for i in range(n):
+            _update_dev(x[i], r[i], p[i], q[i], coef)
 
     def true_residual():
-        ax = apply_all(x)
-        return [b[i] - ax[i] for i in range(n)]
+        """r = b - A x, through the extended vectors (p is kept)."""
+        keep = [t.clone() for t in p]
+        for i in range(n):
+            p[i].copy_(x[i])
+        ax = apply_p()
+        for i in range(n):
+            torch.sub(b[i], ax[i], out=r[i])
+            p[i].copy_(keep[i])
 
-    r = true_residual()
-    bb, rr = dots([(b, b), (r, r)])
+    true_residual()
+    for i in range(n):
+        p[i].copy_(r[i])
+    reduce4(b, r, r)
+    bb, rr = sums.tolist()[:2]
     if not bb > 0.0:
         bb = rr if rr > 0.0 else 1.0
     rel = (rr / bb) ** 0.5
+    thr = rtol * rtol * bb if rtol > 0.0 else -1.0
     it = nrep = 0
     status = 0
-    p = [torch.zeros_like(r[i]) for i in range(n)]
-    beta = 0.0
+    chunk = max(1, int(chunk))
+    g, warm = None, False
     while not (rtol > 0.0 and rel <= rtol) and it < max_iters:
-        for i in range(n):
-            p[i].mul_(beta).add_(r[i])
-        q = apply_all(p)
-        rr_, pq, rq, qq = dots([(r, r), (p, q), (r, q), (q, q)])
-        if not (pq > 0.0) or pq != pq or rr_ != rr_:
+        stop_at = max_iters if replace_every <= 0 else min(max_iters, (it // replace_every + 1) * replace_every)
+        state.copy_(torch.tensor([thr, 0.0, 0.0, float(it), 0.0, float(stop_at)], dtype=torch.float64))
+        while True:
+            # the first chunk runs eagerly (kernels loaded, scratch pools made)
+            if graph and warm and stop_at - it >= chunk:
+                if g is None:
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g):
+                        for _ in range(chunk):
+                            iteration()
+                g.replay()
+            else:
+                for _ in range(min(chunk, stop_at - it)):
+                    iteration()
+                warm = True
+            st = state.tolist()
+            it = int(st[_ITERS])
+            if st[_STOP] != 0.0:
+                break
+        if st[_STOP] == 2.0:
             status = 5
             break
-        alpha = rr_ / pq
+        # stop 1: x and r were updated, p kept -- replace r by the true residual
+        rr_ = st[_RR]
+        true_residual()
+        reduce4(r, r, r)
+        rr_true = sums.tolist()[0]
+        nrep += 1
+        rel = (rr_true / bb) ** 0.5
+        if (rtol > 0.0 and rel <= rtol) or it >= max_iters:
+            break
+        beta = rr_true / rr_ if rr_ > 0.0 else 0.0
         for i in range(n):
-            x[i].add_(p[i], alpha=alpha)
-            r[i].sub_(q[i], alpha=alpha)
-        it += 1
-        rr_next = max(rr_ - 2.0 * alpha * rq + alpha * alpha * qq, 0.0)
-        due = replace_every > 0 and it % replace_every == 0
-        if due or (rtol > 0.0 and rr_next <= rtol * rtol * bb) or it >= max_iters:
-            r = true_residual()
-            (rr_true,) = dots([(r, r)])
-            nrep += 1
-            rel = (rr_true / bb) ** 0.5
-            beta = rr_true / rr_ if rr_ > 0.0 else 0.0
-        else:
-            rel = (rr_next / bb) ** 0.5
-            beta = rr_next / rr_
+            p[i].mul_(beta).add_(r[i])
     if status == 0 and rtol > 0.0 and not rel <= rtol:
         status = 6
     return SlabResult(status, it, nrep, rel)
@@ -236,8 +370,24 @@ class LevinSlab:
         rows = self.store.planes("b")
         return rows[self.skip + self.above:self.skip + self.above + self.R, :self.W].clone()
 
-    def apply(self, x_ext):
+    @property
+    def ext(self):
+        """The extended input vector ((above + R + below) x W): a view of the
+        operator's input buffer, so nothing is copied before a product."""
         n = self.above + self.R + self.below
-        self._x[self.skip:self.skip + n, :self.W].copy_(x_ext)
+        return self._x[self.skip:self.skip + n, :self.W]
+
+    def apply_ext(self):
+        """Own rows (R x W) of the true FP32 operator applied to ext: a view
+        of the output buffer, valid until the next call."""
         self.store.apply(self._x[:, :self.W], self._y[:, :self.W], true_op=True)
+        o = self.skip + self.above
+        return self._y[o:o + self.R, :self.W]
+
+    def apply(self, x_ext):
+        """Extended result (above + R + below) x W of the operator on x_ext
+        (own rows exact, halo rows not)."""
+        self.ext.copy_(x_ext)
+        self.store.apply(self._x[:, :self.W], self._y[:, :self.W], true_op=True)
+        n = self.above + self.R + self.below
         return self._y[self.skip:self.skip + n, :self.W]

@@ -182,6 +182,37 @@ int gm_levin_pad(int W);
 int gm_compute_error(double* mse_host, const float* alpha, const float* gt, int W, int H,
                      void* stream);
 
+/* CG building blocks over pitched row blocks (rows runs of W floats, each
+ * pitch floats apart; device pointers), used by the row-slab solver that
+ * splits one image over several GPUs.  No counterpart in the reference,
+ * which solves one image per process.
+ * gm_cg_dots4: out4 (device, 4 doubles) = FP64 sums of r.r, p.q, r.q, q.q;
+ * the per-block sums are added in block order (deterministic).
+ * gm_cg_update: x += alpha p; r -= alpha q; then p = r + beta p when
+ * update_p is nonzero (FP32, one pass). */
+int gm_cg_dots4(double* out4, const float* r, int r_pitch, const float* p, int p_pitch,
+                const float* q, int q_pitch, int W, int rows, void* stream);
+int gm_cg_update(float* x, int x_pitch, float* r, int r_pitch, float* p, int p_pitch,
+                 const float* q, int q_pitch, int W, int rows, float alpha, float beta,
+                 int update_p, void* stream);
+/* The same iteration with its scalars kept on the device, so a host loop
+ * need not read them back every iteration.  gm_cg_scalars (one thread)
+ * turns the summed sums4 = [r.r, p.q, r.q, q.q] into coef = [alpha, beta,
+ * mode] for gm_cg_update_dev (mode 0: no change, 1: x and r, 2: x, r and p)
+ * and advances state (device, 6 doubles):
+ *   [0] in:  threshold on the recurrence's next r.r (rtol^2 b.b; < 0 none)
+ *   [1] out: r.r of this iteration      [2] out: the recurrence's next r.r
+ *   [3] in/out: iterations taken
+ *   [4] in/out: stop code -- 0 running; 1 the next r.r met the threshold or
+ *       [3] reached [5] (x and r updated, p kept for a residual
+ *       replacement); 2 breakdown (p.q <= 0 or NaN; nothing updated)
+ *   [5] in:  iteration count at which to stop
+ * With a nonzero stop code on entry nothing changes and mode is 0. */
+int gm_cg_scalars(double* coef, double* state, const double* sums4, void* stream);
+int gm_cg_update_dev(float* x, int x_pitch, float* r, int r_pitch, float* p, int p_pitch,
+                     const float* q, int q_pitch, int W, int rows, const double* coef,
+                     void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Native API: Levin store, assembly and solvers                       */
 /* ------------------------------------------------------------------ */

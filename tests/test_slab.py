@@ -34,14 +34,19 @@ class OracleSlab:
         w = O.levin_sym64(image[c0:c1].astype(np.float64) / 255.0, 1e-5)
         self.op = O.Operator(W=Ww, H=c1 - c0, w=w, gamma=gamma[c0:c1].ravel().astype(np.float64))
 
-    def apply(self, x_ext):
+        import torch
+
+        self.ext = torch.zeros((self.above + self.R + self.below, Ww), dtype=torch.float64)
+
+    def apply_ext(self):
         import torch
 
         n = self.above + self.R + self.below
         xc = np.zeros((self.rows, self.W))
-        xc[self.skip:self.skip + n] = x_ext.numpy()
+        xc[self.skip:self.skip + n] = self.ext.numpy()
         y = self.op.apply(xc.ravel()).reshape(self.rows, self.W)
-        return torch.from_numpy(y[self.skip:self.skip + n].copy())
+        o = self.skip + self.above
+        return torch.from_numpy(y[o:o + self.R].copy())
 
 
 def _problem():

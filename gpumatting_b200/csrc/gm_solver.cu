@@ -258,7 +258,7 @@ __device__ __forceinline__ void load_rows(V (&X)[6][6], const V* ring, int r0, i
     }
 }
 
-template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, int KIND, bool PCG = false>
+template <class TLo, int OPLO, int OPHI, bool MIXED, int CFG, int KIND, bool PCG = false, bool FULLW = false>
 __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& geo, unsigned char* smem, int u0,
                                           int v0, int v1, const KState& s, double (&part)[kNPart], Pipe& pp)
 {
@@ -349,7 +349,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     const int c = 8 + kWarpCols * w + 2 * lane;        // smem column of this lane's pixel pair
     const int lc0 = 2 * lane;                          // first operand column (local ring index)
     const int u = u0 + kWarpCols * w + 2 * lane;       // image column of pixel 0
-    const bool in0 = u < geo.W, in1 = u + 1 < geo.W;
+    // FULLW: every column of the strip lies inside the image
+    const bool in0 = FULLW || u < geo.W, in1 = FULLW || u + 1 < geo.W;
     // extra operand pair for the ring halo: lane 0 left, lane 1 right
     const bool has_x = lane < 2;
     const int cx = lane == 0 ? 6 + kWarpCols * w : 8 + kWarpCols * w + kWarpCols;
@@ -359,6 +360,11 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     RingT* ring_d = reinterpret_cast<RingT*>(smem + L.pring_off) + w * OPR * kRingCols;
     float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * OWNR * kWarpCols;  // r or b, own columns
     const int P = A.P;
+    // Krylov outputs, read once from the parameter block (warp-uniform)
+    float* const r_nx = A.r[s.c ^ 1];
+    float* const p_nx = A.p[s.c ^ 1];
+    float* const q_nx = A.q[s.c ^ 1];
+    float* const x_cur = A.xacc[s.xsel];
     constexpr int Rb = K.Rb;
     constexpr bool pcg = PCG && OPLO == OP_SYMD && KIND == KIND_KRYLOV;  // Jacobi-preconditioned CG
 
@@ -369,7 +375,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     uint32_t bw0 = 0u, bw1 = 0u, bw2 = 0u, bw3 = 0u;
 
     auto wait_rec = [&](uint32_t r) {
-        if (!*s_abort && !mbar_wait_bounded(&full[kRvMax + (r & 0xffu)], r >> 8, A.gb, A.tma_limit_ns))
+        if (!mbar_try_wait(&full[kRvMax + (r & 0xffu)], r >> 8) && !*s_abort &&
+            !mbar_wait_bounded(&full[kRvMax + (r & 0xffu)], r >> 8, A.gb, A.tma_limit_ns))
             *s_abort = 1;
     };
     auto band_of = [&](uint32_t r) { return bring + (int)(r & 0xffu) * K.bslot; };
@@ -386,7 +393,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     // row j mod 8 and own ring row j mod 4
     auto phase_a = [&](int j, int vsl, uint32_t vpar) {
         const int Lr = v0 - 2 + j;
-        if (!*s_abort && !mbar_wait_bounded(&full[vsl], vpar, A.gb, A.tma_limit_ns)) *s_abort = 1;
+        if (!mbar_try_wait(&full[vsl], vpar) && !*s_abort && !mbar_wait_bounded(&full[vsl], vpar, A.gb, A.tma_limit_ns))
+            *s_abort = 1;
         const unsigned char* vsp = vring + vsl * K.vslot;
         const bool own_row = Lr >= v0 && Lr < v1;
         const size_t gi = (size_t)(own_row ? Lr : 0) * P + u;
@@ -401,12 +409,10 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             auto combine = [&](int cc, float2& rn, float2& zn, float2& pv) {
                 const float2 rv = ld2(vr, cc);
                 pv = ld2(vp, cc);
-                if (s.skipR) {
-                    rn = rv;
-                } else {
-                    const float2 qv = ld2(vq, cc);
-                    rn = make_float2(fmaf(-s.af, qv.x, rv.x), fmaf(-s.af, qv.y, rv.y));
-                }
+                // selects, not branches (skipR is uniform but costs a branch per row)
+                const float2 qv = ld2(vq, cc);
+                rn.x = s.skipR ? rv.x : fmaf(-s.af, qv.x, rv.x);
+                rn.y = s.skipR ? rv.y : fmaf(-s.af, qv.y, rv.y);
                 if constexpr (pcg) {
                     // d = 0 only outside the image (TMA zero fill), where r = 0 too
                     const float2 dv = ld2(vd, cc);
@@ -420,26 +426,30 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             float2 rn, zn, pv;
             const float2 pn = combine(c, rn, zn, pv);
             *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lc0 + 2) = pn;
-            if (has_x) {
+            {
+                // lanes 0 and 1 also form the ring's halo pairs (left, right);
+                // the other lanes form their own pair again into its own place,
+                // so the warp does not diverge here
                 float2 rx, zx, px;
-                *reinterpret_cast<float2*>(ring_f + rr * kRingCols + lcx) = combine(cx, rx, zx, px);
+                *reinterpret_cast<float2*>(ring_f + rr * kRingCols + (has_x ? lcx : lc0 + 2)) =
+                    combine(has_x ? cx : c, rx, zx, px);
             }
             if (own_row) {
                 *reinterpret_cast<float2*>(own_ring + orow * kWarpCols + lc0) = zn;
                 if (in1) {
-                    *reinterpret_cast<float2*>(A.r[s.c ^ 1] + gi) = rn;
-                    *reinterpret_cast<float2*>(A.p[s.c ^ 1] + gi) = pn;
+                    *reinterpret_cast<float2*>(r_nx + gi) = rn;
+                    *reinterpret_cast<float2*>(p_nx + gi) = pn;
                     if (!s.skipR) {
                         const float2 xv = ld2(vx, c);
-                        *reinterpret_cast<float2*>(A.xacc[s.xsel] + gi) =
+                        *reinterpret_cast<float2*>(x_cur + gi) =
                             make_float2(fmaf(s.af, pv.x, xv.x), fmaf(s.af, pv.y, xv.y));
                     }
                     part[0] += (double)fmaf(rn.x, zn.x, rn.y * zn.y);
                     if constexpr (pcg) part[4] += (double)fmaf(rn.x, rn.x, rn.y * rn.y);
                 } else if (in0) {
-                    A.r[s.c ^ 1][gi] = rn.x;
-                    A.p[s.c ^ 1][gi] = pn.x;
-                    if (!s.skipR) A.xacc[s.xsel][gi] = fmaf(s.af, pv.x, vx[c]);
+                    r_nx[gi] = rn.x;
+                    p_nx[gi] = pn.x;
+                    if (!s.skipR) x_cur[gi] = fmaf(s.af, pv.x, vx[c]);
                     part[0] += (double)rn.x * (double)zn.x;
                     if constexpr (pcg) part[4] += (double)rn.x * (double)rn.x;
                 }
@@ -606,26 +616,27 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         }
                     }
                     if (in1) {
-                        *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go) = q0;
+                        *reinterpret_cast<float2*>(q_nx + go) = q0;
                         float spq = fmaf(X[2][2], q0.x, X[2][3] * q0.y);
                         float srq = fmaf(rn0.x, q0.x, rn0.y * q0.y);
                         float sqq = fmaf(q0.x * w0.x, q0.x, q0.y * w0.y * q0.y);
                         if (second) {
-                            *reinterpret_cast<float2*>(A.q[s.c ^ 1] + go + P) = q1;
-                            part[1] += (double)fmaf(X[3][2], q1.x, X[3][3] * q1.y);
-                            part[2] += (double)fmaf(rn1.x, q1.x, rn1.y * q1.y);
-                            part[3] += (double)fmaf(q1.x * w1.x, q1.x, q1.y * w1.y * q1.y);
+                            // both rows' products in FP32, one FP64 add per sum
+                            *reinterpret_cast<float2*>(q_nx + go + P) = q1;
+                            spq = fmaf(X[3][2], q1.x, fmaf(X[3][3], q1.y, spq));
+                            srq = fmaf(rn1.x, q1.x, fmaf(rn1.y, q1.y, srq));
+                            sqq = fmaf(q1.x * w1.x, q1.x, fmaf(q1.y * w1.y, q1.y, sqq));
                         }
                         part[1] += (double)spq;
                         part[2] += (double)srq;
                         part[3] += (double)sqq;
                     } else {
-                        A.q[s.c ^ 1][go] = q0.x;
+                        q_nx[go] = q0.x;
                         part[1] += (double)X[2][2] * (double)q0.x;
                         part[2] += (double)rn0.x * (double)q0.x;
                         part[3] += (double)q0.x * w0.x * (double)q0.x;
                         if (second) {
-                            A.q[s.c ^ 1][go + P] = q1.x;
+                            q_nx[go + P] = q1.x;
                             part[1] += (double)X[3][2] * (double)q1.x;
                             part[2] += (double)rn1.x * (double)q1.x;
                             part[3] += (double)q1.x * w1.x * (double)q1.x;
@@ -936,9 +947,18 @@ __global__ void __launch_bounds__(cfg_threads(CFG), solver_min_blocks<TLo, OPLO,
         for (int piece = 0; piece < (BATCH ? 2 : 1); ++piece) {
             const int pu0 = piece ? u0b : u0, pv0 = piece ? v0b : v0, pv1 = piece ? v1b : v1;
             if (!(pv1 > pv0) || done) continue;
-            if (kind == KIND_KRYLOV && pcg_mode)
+            // every strip of the image full: one code path for the whole grid
+            // (a grid that mixes both paths on one SM runs slower)
+            const bool fullw = !BATCH && geo.W % cfg_strip(CFG) == 0;
+            if (kind == KIND_KRYLOV && pcg_mode && fullw)
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV, OPLO == OP_SYMD, true>(A, geo, smem, pu0, pv0, pv1,
+                                                                                          s, part, pp);
+            else if (kind == KIND_KRYLOV && pcg_mode)
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV, OPLO == OP_SYMD>(A, geo, smem, pu0, pv0, pv1, s,
                                                                                     part, pp);
+            else if (kind == KIND_KRYLOV && fullw)
+                run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV, false, true>(A, geo, smem, pu0, pv0, pv1, s, part,
+                                                                                 pp);
             else if (kind == KIND_KRYLOV)
                 run_sweep<TLo, OPLO, OPHI, MIXED, CFG, KIND_KRYLOV>(A, geo, smem, pu0, pv0, pv1, s, part, pp);
             else if (kind == KIND_REPLACE)

@@ -134,6 +134,34 @@ def test_levin_solve_accurate_vs_direct(orc):
     assert np.abs(alpha.double().cpu().numpy().ravel() - xs).max() <= TOL
 
 
+@pytest.mark.parametrize("W,strip,solver", [(384, 192, "cg"), (384, 192, "pcg"), (256, 128, "cg"), (383, 192, "cg")])
+def test_full_strip_widths_accurate_vs_direct(orc, W, strip, solver):
+    """Widths that are a whole number of strips take the kernel's full-strip
+    path (no per-lane column tests); both paths agree with the FP64 direct
+    solve to 1e-4 at rel-res 1e-10."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    torch = torch_cuda()
+    H = 40
+    api, st, p, w, g, b = _store(orc, W, H, "fp16", seed=7)
+    a = orc.sym_to_bands64(w, g, W, H)
+    offs = orc.levin_offsets(W)
+    N = W * H
+    rows, cols, vals = [], [], []
+    for k in range(25):
+        i = np.arange(N)
+        j = i + offs[k]
+        m = (j >= 0) & (j < N) & (a[k] != 0)
+        rows.append(i[m]); cols.append(j[m]); vals.append(a[k][m])
+    M = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+    xs = spla.spsolve(M.tocsc(), b)
+    alpha = torch.full((H, W), 0.5, device="cuda")
+    res = st.solve(alpha, solver, rtol=1e-10, max_iters=50000, strip_width=strip)
+    assert res.status == 0 and res.rel_residual <= 1e-10, res
+    assert np.abs(alpha.double().cpu().numpy().ravel() - xs).max() <= TOL
+
+
 def test_levin_gd_and_jacobi_fixed_iterations(orc):
     torch = torch_cuda()
     W, H = 96, 64

@@ -621,11 +621,19 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                         float srq = fmaf(rn0.x, q0.x, rn0.y * q0.y);
                         float sqq = fmaf(q0.x * w0.x, q0.x, q0.y * w0.y * q0.y);
                         if (second) {
-                            // both rows' products in FP32, one FP64 add per sum
                             *reinterpret_cast<float2*>(q_nx + go + P) = q1;
-                            spq = fmaf(X[3][2], q1.x, fmaf(X[3][3], q1.y, spq));
-                            srq = fmaf(rn1.x, q1.x, fmaf(rn1.y, q1.y, srq));
-                            sqq = fmaf(q1.x * w1.x, q1.x, fmaf(q1.y * w1.y, q1.y, sqq));
+                            if constexpr (OPLO == OP_SYMD) {
+                                // both rows' products in FP32, one FP64 add per sum
+                                spq = fmaf(X[3][2], q1.x, fmaf(X[3][3], q1.y, spq));
+                                srq = fmaf(rn1.x, q1.x, fmaf(rn1.y, q1.y, srq));
+                                sqq = fmaf(q1.x * w1.x, q1.x, fmaf(q1.y * w1.y, q1.y, sqq));
+                            } else {
+                                // the plain FP32 method (the reference's layout) keeps
+                                // one FP64 add per row and partial sum
+                                part[1] += (double)fmaf(X[3][2], q1.x, X[3][3] * q1.y);
+                                part[2] += (double)fmaf(rn1.x, q1.x, rn1.y * q1.y);
+                                part[3] += (double)fmaf(q1.x * w1.x, q1.x, q1.y * w1.y * q1.y);
+                            }
                         }
                         part[1] += (double)spq;
                         part[2] += (double)srq;

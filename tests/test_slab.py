@@ -23,7 +23,7 @@ W, H, SEED = 48, 41, 3
 class OracleSlab:
     """FP64 CPU stand-in for a slab operator (test infrastructure)."""
 
-    def __init__(self, image, gamma, r0, r1):
+    def __init__(self, image, gamma, r0, r1, pitched=False):
         from oracle import oracle as O
 
         Hh, Ww = gamma.shape
@@ -36,7 +36,11 @@ class OracleSlab:
 
         import torch
 
-        self.ext = torch.zeros((self.above + self.R + self.below, Ww), dtype=torch.float64)
+        n = self.above + self.R + self.below
+        # pitched: a view into rows wider than W, as the GPU slab's buffer is
+        # when W is not a multiple of 4 (its halo rows are not contiguous)
+        self.ext = (torch.zeros((n, Ww + 3), dtype=torch.float64)[:, :Ww] if pitched
+                    else torch.zeros((n, Ww), dtype=torch.float64))
 
     def apply_ext(self):
         import torch
@@ -66,7 +70,7 @@ def _single_domain(rtol):
     return x.reshape(H, W), it, op
 
 
-def _solve_slabs(nslabs, first, count, rtol=1e-11):
+def _solve_slabs(nslabs, first, count, rtol=1e-11, pitched=False):
     import torch
 
     p, g, b = _problem()
@@ -74,7 +78,7 @@ def _solve_slabs(nslabs, first, count, rtol=1e-11):
     slabs, xs, bs = [], [], []
     for k in range(first, first + count):
         r0, r1 = S.slab_bounds(H, nslabs, k)
-        slabs.append(OracleSlab(p.image, g, r0, r1))
+        slabs.append(OracleSlab(p.image, g, r0, r1, pitched))
         xs.append(torch.full((r1 - r0, W), 0.5, dtype=torch.float64))
         bs.append(torch.from_numpy(b[r0:r1].copy()))
     comm = S.SlabComm(nslabs, first, count)
@@ -115,7 +119,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, q, nslabs, mode):
+def _rank_main(rank, world, port, q, nslabs, mode, pitched=False):
     import datetime
 
     import torch.distributed as dist
@@ -128,7 +132,7 @@ def _rank_main(rank, world, port, q, nslabs, mode):
             q.put((rank, "left"))
             return
         try:
-            res, xs = _solve_slabs(nslabs, first, count)
+            res, xs = _solve_slabs(nslabs, first, count, pitched=pitched)
             q.put((rank, res, first, xs))
         except Exception as e:  # noqa: BLE001 - a failed exchange is the expected outcome of "leave"
             q.put((rank, "error", type(e).__name__))
@@ -137,11 +141,11 @@ def _rank_main(rank, world, port, q, nslabs, mode):
             dist.destroy_process_group()
 
 
-def _run(nslabs, mode="ok"):
+def _run(nslabs, mode="ok", pitched=False):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q, nslabs, mode)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q, nslabs, mode, pitched)) for r in range(2)]
     for p in procs:
         p.start()
     out = [q.get(timeout=300) for _ in range(2)]
@@ -152,14 +156,15 @@ def _run(nslabs, mode="ok"):
     return sorted(out, key=lambda o: o[0])
 
 
-@pytest.mark.parametrize("nslabs", [2, 4])
-def test_two_gloo_ranks_solve_one_image(nslabs):
+@pytest.mark.parametrize("nslabs,pitched", [(2, False), (4, False), (2, True)])
+def test_two_gloo_ranks_solve_one_image(nslabs, pitched):
     """Two ranks (one or two slabs each), halo rows over gloo send/recv and
     one all-reduce per iteration: the gathered solution matches the
     single-domain FP64 CG within 1e-6 relative, and both ranks agree on the
-    iteration count and residual."""
+    iteration count and residual.  pitched: the halo rows travel through
+    contiguous staging tensors."""
     x64, it64, op = _single_domain(1e-11)
-    out = _run(nslabs)
+    out = _run(nslabs, pitched=pitched)
     (_, r0, f0, xs0), (_, r1, f1, xs1) = out
     assert r0 == r1 and r0.status == 0 and r0.rel_residual <= 1e-11, (r0, r1)
     x = np.concatenate(xs0 + xs1)

@@ -276,6 +276,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     unsigned char* bring = smem + K.bbase;
     volatile int* s_abort = reinterpret_cast<volatile int*>(smem + L.red_off + cfg_red_bytes(CFG));
     constexpr bool kSymBand = (KIND == KIND_KRYLOV ? OPLO : OPHI) != OP_REF25;
+    constexpr bool kEarly = kSymBand && KIND != KIND_KRYLOV;
 
     if (warp == NCONS) {
         // ------------------------------ producer ------------------------------
@@ -574,7 +575,7 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                     wait_rec(bw1);
                 }
                 wait_rec(bw2);
-                if (second) wait_rec(bw3);
+                if (second && !kEarly) wait_rec(bw3);  // early release: waited before row v + 1
             } else {
                 wait_rec(bw2);
                 if (second) wait_rec(bw3);
@@ -585,6 +586,76 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
             const int o0 = (j - 2) & (OWNR - 1);  // own ring row of output row v
             const int o1 = (j - 1) & (OWNR - 1);
             const size_t go = (size_t)v * P + u;
+            // The rows of a replacement or Jacobi sweep (r0_: output row v,
+            // r1_: row v + 1), each call loading the operand window itself.
+            auto nk_rows = [&](bool r0_, bool r1_) {
+                if constexpr (KIND == KIND_REPLACE) {
+                    double X[6][6];
+                    if constexpr (MIXED) {
+                        load_rows<double, OPR>(X, ring_d, r0, lc0);
+                    } else {
+                        float Xf[6][6];
+                        load_rows<float, OPR>(Xf, ring_d, r0, lc0);
+#pragma unroll
+                        for (int a = 0; a < 6; ++a)
+#pragma unroll
+                            for (int b2 = 0; b2 < 6; ++b2) X[a][b2] = (double)Xf[a][b2];
+                    }
+                    auto rep_row = [&](double y0, double y1, const float2 bv, size_t g, int vr, int ro) {
+                        const float r0f = (float)((double)bv.x - y0), r1f = (float)((double)bv.y - y1);
+                        float* ao = geo.aout + (size_t)(vr - geo.arow0) * geo.apitch + u;
+                        ao[0] = (float)X[ro + 2][2];
+                        A.r[s.c][g] = r0f;
+                        part[0] += (double)r0f * (double)r0f;
+                        part[1] += (double)bv.x * (double)bv.x;
+                        if (in1) {
+                            ao[1] = (float)X[ro + 2][3];
+                            A.r[s.c][g + 1] = r1f;
+                            part[0] += (double)r1f * (double)r1f;
+                            part[1] += (double)bv.y * (double)bv.y;
+                        }
+                    };
+                    double y0, y1, d0, d1;
+                    if (r0_) {
+                        if (OPHI == OP_REF25) ref25_apply<double, 0, BOX>(y0, y1, d0, d1, X, bA[0], c);
+                        else symi_apply<double, 0, BOX>(y0, y1, d0, d1, X, bA, K.xoff, c);
+                        rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, v, 0);
+                    }
+                    if (r1_) {
+                        if (OPHI == OP_REF25) ref25_apply<double, 1, BOX>(y0, y1, d0, d1, X, bB[0], c);
+                        else symi_apply<double, 1, BOX>(y0, y1, d0, d1, X, bB, K.xoff, c);
+                        rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0), go + P,
+                                v + 1, 1);
+                    }
+                } else if constexpr (KIND == KIND_JACOBI) {
+                    float X[6][6];
+                    load_rows<float, OPR>(X, ring_f, r0, lc0);
+                    auto jac_row = [&](float y0, float y1, float d0, float d1, const float2 bv, size_t g, int ro) {
+                        const float rv0 = bv.x - y0, rv1 = bv.y - y1;
+                        A.xacc[s.xsel ^ 1][g] = X[ro + 2][2] + A.omega * rv0 / d0;
+                        part[0] += (double)rv0 * (double)rv0;
+                        part[1] += (double)bv.x * (double)bv.x;
+                        if (in1) {
+                            A.xacc[s.xsel ^ 1][g + 1] = X[ro + 2][3] + A.omega * rv1 / d1;
+                            part[0] += (double)rv1 * (double)rv1;
+                            part[1] += (double)bv.y * (double)bv.y;
+                        }
+                    };
+                    float y0, y1, d0, d1;
+                    if (r0_) {
+                        if (OPHI == OP_REF25) ref25_apply<float, 0, BOX>(y0, y1, d0, d1, X, bA[0], c);
+                        else symi_apply<float, 0, BOX>(y0, y1, d0, d1, X, bA, K.xoff, c);
+                        jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go,
+                                0);
+                    }
+                    if (r1_) {
+                        if (OPHI == OP_REF25) ref25_apply<float, 1, BOX>(y0, y1, d0, d1, X, bB[0], c);
+                        else symi_apply<float, 1, BOX>(y0, y1, d0, d1, X, bB, K.xoff, c);
+                        jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0),
+                                go + P, 1);
+                    }
+                }
+            };
             if (in0) {
                 if (KIND == KIND_KRYLOV) {
                     float X[6][6];
@@ -650,73 +721,27 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
                             part[3] += (double)q1.x * w1.x * (double)q1.x;
                         }
                     }
-                } else if (KIND == KIND_REPLACE) {
-                    double X[6][6];
-                    if constexpr (MIXED) {
-                        load_rows<double, OPR>(X, ring_d, r0, lc0);
-                    } else {
-                        float Xf[6][6];
-                        load_rows<float, OPR>(Xf, ring_d, r0, lc0);
-#pragma unroll
-                        for (int a = 0; a < 6; ++a)
-#pragma unroll
-                            for (int b2 = 0; b2 < 6; ++b2) X[a][b2] = (double)Xf[a][b2];
-                    }
-                    auto rep_row = [&](double y0, double y1, const float2 bv, size_t g, int vr, int ro) {
-                        const float r0f = (float)((double)bv.x - y0), r1f = (float)((double)bv.y - y1);
-                        float* ao = geo.aout + (size_t)(vr - geo.arow0) * geo.apitch + u;
-                        ao[0] = (float)X[ro + 2][2];
-                        A.r[s.c][g] = r0f;
-                        part[0] += (double)r0f * (double)r0f;
-                        part[1] += (double)bv.x * (double)bv.x;
-                        if (in1) {
-                            ao[1] = (float)X[ro + 2][3];
-                            A.r[s.c][g + 1] = r1f;
-                            part[0] += (double)r1f * (double)r1f;
-                            part[1] += (double)bv.y * (double)bv.y;
-                        }
-                    };
-                    double y0, y1, d0, d1;
-                    if (OPHI == OP_REF25) ref25_apply<double, 0, BOX>(y0, y1, d0, d1, X, bA[0], c);
-                    else symi_apply<double, 0, BOX>(y0, y1, d0, d1, X, bA, K.xoff, c);
-                    rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, v, 0);
-                    if (second) {
-                        if (OPHI == OP_REF25) ref25_apply<double, 1, BOX>(y0, y1, d0, d1, X, bB[0], c);
-                        else symi_apply<double, 1, BOX>(y0, y1, d0, d1, X, bB, K.xoff, c);
-                        rep_row(y0, y1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0), go + P,
-                                v + 1, 1);
-                    }
-                } else {  // Jacobi
-                    float X[6][6];
-                    load_rows<float, OPR>(X, ring_f, r0, lc0);
-                    auto jac_row = [&](float y0, float y1, float d0, float d1, const float2 bv, size_t g, int ro) {
-                        const float rv0 = bv.x - y0, rv1 = bv.y - y1;
-                        A.xacc[s.xsel ^ 1][g] = X[ro + 2][2] + A.omega * rv0 / d0;
-                        part[0] += (double)rv0 * (double)rv0;
-                        part[1] += (double)bv.x * (double)bv.x;
-                        if (in1) {
-                            A.xacc[s.xsel ^ 1][g + 1] = X[ro + 2][3] + A.omega * rv1 / d1;
-                            part[0] += (double)rv1 * (double)rv1;
-                            part[1] += (double)bv.y * (double)bv.y;
-                        }
-                    };
-                    float y0, y1, d0, d1;
-                    if (OPHI == OP_REF25) ref25_apply<float, 0, BOX>(y0, y1, d0, d1, X, bA[0], c);
-                    else symi_apply<float, 0, BOX>(y0, y1, d0, d1, X, bA, K.xoff, c);
-                    jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o0 * kWarpCols + lc0), go, 0);
-                    if (second) {
-                        if (OPHI == OP_REF25) ref25_apply<float, 1, BOX>(y0, y1, d0, d1, X, bB[0], c);
-                        else symi_apply<float, 1, BOX>(y0, y1, d0, d1, X, bB, K.xoff, c);
-                        jac_row(y0, y1, d0, d1, *reinterpret_cast<const float2*>(own_ring + o1 * kWarpCols + lc0),
-                                go + P, 1);
-                    }
+                } else {
+                    nk_rows(true, second && !kEarly);
+                }
+            }
+            if constexpr (kEarly) {
+                // band row v - 2 is read by output row v only: its slot goes
+                // back before row v + 1 is formed, so that the producer refills
+                // it meanwhile (this kind's four band slots are exactly the two
+                // rows' window and leave no room to load ahead otherwise)
+                __syncwarp();
+                release_rec(bw0);
+                if (second) {
+                    wait_rec(bw3);
+                    if (in0) nk_rows(false, true);
                 }
             }
             __syncwarp();
             // band steps read for the last time: j-4, j-3 (symmetric store)
             // and, at the last super-step, the rest
             if (kSymBand) {
-                release_rec(bw0);
+                if (!kEarly) release_rec(bw0);
                 release_rec(bw1);
                 if (j + 2 >= nsteps) {
                     release_rec(bw2);

@@ -297,6 +297,9 @@ def cg_scalars(coef, state, sums4, stream=None):
     """One thread on the device: coef = [alpha, beta, mode] from the summed
     sums4 = [r.r, p.q, r.q, q.q], advancing the 6-double device state
     (threshold, r.r, next r.r, iterations, stop code, stop-at count)."""
+    torch = _torch()
+    if not isinstance(sums4, torch.Tensor):
+        raise TypeError("sums4 must be a float64 CUDA tensor")
     _f64_dev(sums4, 4, "sums4", sums4.device)
     _f64_dev(coef, 3, "coef", sums4.device)
     _f64_dev(state, 6, "state", sums4.device)

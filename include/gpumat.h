@@ -189,7 +189,7 @@ int gm_compute_error(double* mse_host, const float* alpha, const float* gt, int 
  * gm_cg_dots4: out4 (device, 4 doubles) = FP64 sums of r.r, p.q, r.q, q.q;
  * the per-block sums are added in block order (deterministic).
  * gm_cg_update: x += alpha p; r -= alpha q; then p = r + beta p when
- * update_p is nonzero (FP32, one pass). */
+ * update_p is nonzero (FP32, one pass).  The four blocks must not overlap. */
 int gm_cg_dots4(double* out4, const float* r, int r_pitch, const float* p, int p_pitch,
                 const float* q, int q_pitch, int W, int rows, void* stream);
 int gm_cg_update(float* x, int x_pitch, float* r, int r_pitch, float* p, int p_pitch,

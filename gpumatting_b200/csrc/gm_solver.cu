@@ -357,8 +357,8 @@ __device__ __forceinline__ void run_sweep(const SolverArgs& A, const UnitGeo& ge
     const int cx = lane == 0 ? 6 + kWarpCols * w : 8 + kWarpCols * w + kWarpCols;
     const int lcx = lane == 0 ? 0 : kRingCols - 2;
     using RingT = std::conditional_t<MIXED, double, float>;  // replacement operand ring element
-    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * OPR * kRingCols * (MIXED ? 2 : 1);
-    RingT* ring_d = reinterpret_cast<RingT*>(smem + L.pring_off) + w * OPR * kRingCols;
+    float* ring_f = reinterpret_cast<float*>(smem + L.pring_off) + w * OPR * kRingCols;
+    RingT* ring_d = reinterpret_cast<RingT*>(smem + L.pringd_off) + w * OPR * kRingCols;
     float* own_ring = reinterpret_cast<float*>(smem + L.rring_off) + w * OWNR * kWarpCols;  // r or b, own columns
     const int P = A.P;
     // Krylov outputs, read once from the parameter block (warp-uniform)

@@ -99,10 +99,13 @@ __host__ __device__ constexpr KindLayout kind_layout(int kind, int op, int esize
 // slots and (symmetric store) four band slots, so Rv >= 2 and Rb >= 4 (2 for
 // the reference layout) always make progress; extra slots are prefetch.
 // Configs 0 and 2 fit three (four) CTAs per SM with a 2-byte store, config 1
-// trades one CTA per SM for rings about twice as deep.
+// trades one CTA per SM for rings about twice as deep.  Config 0's fifth
+// Krylov vector slot is the room the replacement sweep's operand ring leaves
+// by overlapping the Krylov rings (make_layout).
 __host__ __device__ constexpr int rings_v(int kind, int oplo, int cfg)
 {
-    return kind == KIND_KRYLOV ? (cfg == 1 && oplo == OP_SYMD ? 8 : 4) : (cfg == 1 && oplo == OP_SYMD ? 3 : 2);
+    return kind == KIND_KRYLOV ? (cfg == 1 && oplo == OP_SYMD ? 8 : cfg == 0 && oplo == OP_SYMD ? 5 : 4)
+                               : (cfg == 1 && oplo == OP_SYMD ? 3 : 2);
 }
 __host__ __device__ constexpr int rings_b(int kind, int oplo, int cfg)
 {
@@ -117,7 +120,7 @@ __host__ __device__ constexpr int ring_esize(bool mixed) { return mixed ? 8 : 4;
 // The vector and band rings of a sweep share one area whose split depends on
 // the sweep kind (a sweep starts with both rings drained).
 struct Layout {
-    int ring_bytes, pring_off, rring_off, full_off, empty_off, red_off, total;
+    int ring_bytes, pring_off, pringd_off, rring_off, full_off, empty_off, red_off, total;
     KindLayout k[NKIND];
 };
 
@@ -130,11 +133,19 @@ __host__ __device__ constexpr Layout make_layout(int oplo, int esize_lo, int oph
     for (int k = 0; k < NKIND; ++k)
         L.k[k] = kind_layout(k, k == KIND_KRYLOV ? oplo : ophi, k == KIND_KRYLOV ? esize_lo : 4, mixed,
                              rings_v(k, oplo, cfg), rings_b(k, oplo, cfg), box);
-    int cap = 0;
-    for (int k = 0; k < NKIND; ++k) cap = imax(cap, L.k[k].bbase + L.k[k].Rb * L.k[k].bslot);
-    L.ring_bytes = a128(cap);
-    L.pring_off = L.ring_bytes;
-    L.rring_off = L.pring_off + a128(ncol * kOpRows * kRingCols * ring_esize(mixed));
+    int cap[NKIND] = {};
+    for (int k = 0; k < NKIND; ++k) cap[k] = L.k[k].bbase + L.k[k].Rb * L.k[k].bslot;
+    L.ring_bytes = a128(imax(cap[KIND_KRYLOV], imax(cap[KIND_REPLACE], cap[KIND_JACOBI])));
+    // Operand rings: the float one (Krylov and Jacobi sweeps) after the larger
+    // of those kinds' TMA rings; the replacement sweep's (FP64 when mixed)
+    // after its own TMA rings, where it may overlap the Krylov rings and the
+    // float ring, which a replacement sweep does not use (every load of a
+    // sweep has landed and been read before the next sweep starts).
+    const int pf = a128(ncol * kOpRows * kRingCols * 4);
+    const int pd = a128(ncol * kOpRows * kRingCols * ring_esize(mixed));
+    L.pring_off = a128(imax(cap[KIND_KRYLOV], cap[KIND_JACOBI]));
+    L.pringd_off = a128(cap[KIND_REPLACE]);
+    L.rring_off = imax(L.pring_off + pf, L.pringd_off + pd);
     L.full_off = L.rring_off + a128(ncol * kOwnRows * kWarpCols * 4);
     L.empty_off = L.full_off + a128((kRvMax + kRbMax) * 8);
     L.red_off = L.empty_off + a128((kRvMax + kRbMax) * 8);

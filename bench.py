@@ -563,7 +563,7 @@ def run_ours(args):
         pl = run_plain(args, prob, img_d, scr_d, flush, stream, mixed_once)
         pl["speedup_mixed_vs_plain"] = pl["speedup_median"]
         pl["speedup_mixed_step_vs_plain_solve"] = pl["ms_per_solve"] / line["ms_per_step"]
-        # the north-star target numbers, where a reader of the line sees them first
+        # the mixed-vs-plain target numbers, where a reader of the line sees them first
         line["speedup_mixed_vs_plain"] = pl["speedup_median"]
         line["speedup_mixed_vs_plain_range"] = [pl["speedup_per_round_min"], pl["speedup_per_round_max"]]
         line["plain_fp32_ms"] = pl["ms_per_solve"]
